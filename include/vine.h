@@ -1,0 +1,204 @@
+/*
+ * vine.h -- C ABI of the B200 exact constrained-shortest-path (CSP) engine.
+ *
+ * Problem (the reference's CSP=1 instance): a label is a partial path
+ * (vid, d, delay) from the source; expanding it over arc (u -> v, len, dly)
+ * gives (v, d + len, delay + dly) (include/label.hpp:214-222); label a
+ * dominates b when a.d <= b.d and a.delay <= b.delay
+ * (include/label.hpp:234-236); a label is feasible when !(delay > budget)
+ * (include/constraint.hpp:99-101).  A query asks for the feasible
+ * source -> sink path of smallest cost d; ties are broken by smaller delay,
+ * so the answer (cost, delay) is unique.
+ *
+ * The reference binds this path only through C++ templates -- the query class
+ * cspp<Label_t, Edge_t> (algorithm/cspp.hpp:11-69) and its GPU driver
+ * RUN_CSPP (algorithm/cspp.cuh:50-58, 69-325).  Each entry point below names
+ * the reference interface it replaces.  include/vine/cspp.hpp layers the
+ * reference's class shape on top of these functions.
+ *
+ * Conventions: every function returns a vine_status (0 = VINE_OK, negative =
+ * error); no C++ exception crosses this boundary; output buffers are owned by
+ * the caller; the last error message of the calling thread is available from
+ * vine_last_error().  Weights must be finite and >= 0.  Optimal costs are
+ * bit-exact (the same FP32 additions along the same path as the reference)
+ * whenever the weights are integers whose path sums stay below 2^24.
+ */
+#ifndef VINE_H_
+#define VINE_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  VINE_OK = 0,
+  VINE_ERR_INVALID = -1,   /* bad argument                                   */
+  VINE_ERR_CAPACITY = -2,  /* a label pool / pile / table / output overflowed */
+  VINE_ERR_CUDA = -3,      /* CUDA runtime error                             */
+  VINE_ERR_TIMEOUT = -4,   /* a bounded device wait gave up                  */
+  VINE_ERR_NO_DEVICE = -5, /* no usable CUDA device                          */
+  VINE_ERR_IO = -6,        /* file could not be read / parsed                */
+  VINE_ERR_INTERNAL = -7
+} vine_status;
+
+/* Thread-local text of the last error (never NULL). */
+const char *vine_last_error(void);
+/* Library version string. */
+const char *vine_version(void);
+
+/* ------------------------------------------------------------------ graph */
+
+typedef struct vine_graph vine_graph;
+
+/* Uploads a CSR graph to `device` (SoA: row_ptr[n+1], col[m], len[m],
+ * delay[m]; arcs of vertex u are col[row_ptr[u] .. row_ptr[u+1])).  Also
+ * builds the reverse CSR used by the lower-bound searches.
+ * Replaces Graph::adj_to_csr + Graph::make_gpu_graph
+ * (include/graph.hpp:136-195) and the gpuGraph device struct
+ * (include/gpu_graph.hpp:5-35). */
+int vine_graph_create(int32_t device, int32_t n, int64_t m, const int64_t *row_ptr,
+                      const int32_t *col, const float *len, const float *delay,
+                      vine_graph **out);
+void vine_graph_destroy(vine_graph *g);
+/* n, m, and 1 when every weight is an integer < 2^24 (exactness regime). */
+int vine_graph_info(const vine_graph *g, int32_t *n, int64_t *m, int32_t *integral);
+
+/* ----------------------------------------------------------------- config */
+
+enum vine_engine {
+  VINE_ENGINE_BATCH = 0, /* persistent kernel, one query per CTA worker     */
+  VINE_ENGINE_PLAIN = 1  /* one query at a time, whole GPU, host-driven     */
+};
+enum vine_mode {
+  VINE_MODE_OPTIMAL = 0, /* prune by the incumbent; answer = lex-min label  */
+  VINE_MODE_PARETO = 1   /* no incumbent / bounds: full sink Pareto set     */
+};
+enum vine_policy {
+  VINE_POLICY_FIXED = 0, /* constant bucket width                           */
+  VINE_POLICY_AR = 1,    /* AR(3) (Burg) forecast of the frontier size      */
+  VINE_POLICY_MLP = 2    /* learned 16-64-64-2 scheduler (needs cfg.mlp)    */
+};
+
+typedef struct vine_mlp vine_mlp;
+
+typedef struct {
+  int32_t engine;          /* vine_engine                                     */
+  int32_t mode;            /* vine_mode                                       */
+  int32_t policy;          /* vine_policy                                     */
+  int32_t use_bounds;      /* reverse lower bounds (delay and A* cost)        */
+  int32_t block_threads;   /* batch engine: threads per query worker (CTA)    */
+  int32_t ctas_per_sm;     /* batch engine: resident workers per SM (0=auto)  */
+  int32_t table_log2;      /* shared-memory bucket table entries (log2)       */
+  int32_t spill_log2;      /* per-worker HBM spill table entries (log2)       */
+  float bucket_width;      /* bucket width in cost units (0 = auto)           */
+  int32_t split_threshold; /* max labels expanded per round (0 = auto)        */
+  int64_t pool_labels;     /* label arena capacity (0 = auto)                 */
+  int64_t far_capacity;    /* per-worker far-pile entries (0 = auto)          */
+  int32_t use_cuda_graph;  /* replay the batch launch sequence as a graph     */
+  int32_t order_queries;   /* batch engine: largest budget first              */
+  const vine_mlp *mlp;     /* model for VINE_POLICY_MLP                       */
+  int32_t trace;           /* record per-bucket scheduler traces              */
+  int32_t reserved[7];
+} vine_config;
+
+void vine_config_default(vine_config *cfg);
+
+/* ---------------------------------------------------------------- results */
+
+enum vine_stat {
+  VINE_STAT_EXPANDED = 0, /* labels popped and expanded                      */
+  VINE_STAT_RELAXED,      /* arcs relaxed                                    */
+  VINE_STAT_INSERTED,     /* labels accepted into a store / pile             */
+  VINE_STAT_DOMINATED,    /* candidates rejected by dominance                */
+  VINE_STAT_BUCKETS,      /* buckets processed                               */
+  VINE_STAT_ROUNDS,       /* expansion rounds                                */
+  VINE_STAT_SPILLS,       /* labels placed in the HBM spill table            */
+  VINE_STAT_CYCLES,       /* device clock cycles spent on the query          */
+  VINE_STAT_COUNT = 8
+};
+
+typedef struct {
+  float *cost;            /* [nq] optimal cost (+inf when infeasible)        */
+  float *delay;           /* [nq] delay of that path                         */
+  int32_t *found;         /* [nq] 1 = feasible path exists                   */
+  int32_t *status;        /* [nq] per-query vine_status                      */
+  int64_t *path_offsets;  /* [nq+1] or NULL: path of q is                    */
+  int32_t *path;          /*   path[path_offsets[q] .. path_offsets[q+1])    */
+  int64_t path_capacity;  /*   capacity of `path` in vertices                */
+  float *pareto_d;        /* [nq*pareto_stride] or NULL (VINE_MODE_PARETO)  */
+  float *pareto_delay;    /* [nq*pareto_stride]                              */
+  int32_t *pareto_n;      /* [nq] size of the sink Pareto set                */
+  int32_t pareto_stride;
+  int64_t *stats;         /* [nq*VINE_STAT_COUNT] or NULL                    */
+} vine_results;
+
+/* Solves nq queries (source src[q], sink dst[q], delay budget budget[q]) from
+ * HOST buffers; copies in, runs, copies results out.  Replaces
+ * cspp<c_label,c_edge>::solve (algorithm/cspp.hpp:48-53) -> RUN_CSPP
+ * (algorithm/cspp.cuh:69-325), which returned nothing; this fills cost,
+ * delay, path and (in Pareto mode) the sink's Pareto set.  A query whose
+ * status is VINE_ERR_CAPACITY is re-run once with larger pools before the
+ * call gives up.  Returns the first per-query error, or VINE_OK. */
+int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst,
+               const float *budget, const vine_config *cfg, vine_results *out);
+
+/* Device-resident variant: src/dst/budget and every output pointer are device
+ * pointers, work is enqueued on `stream` (cudaStream_t, may be NULL) and the
+ * call returns without waiting.  out->path / path_offsets must be device
+ * buffers sized by the caller (path_capacity); paths are packed in completion
+ * order and path_offsets[q] holds the start, out->stats etc. as above.
+ * Not retried on capacity errors. */
+int vine_solve_device(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst,
+                      const float *budget, const vine_config *cfg, vine_results *out,
+                      void *stream);
+
+/* ------------------------------------------------------- learned scheduler */
+
+#define VINE_MLP_IN 16
+#define VINE_MLP_HIDDEN 64
+#define VINE_MLP_OUT 2
+/* Number of FP32 parameters: W1[64x16] b1[64] W2[64x64] b2[64] W3[2x64] b3[2]. */
+#define VINE_MLP_PARAMS (64 * 16 + 64 + 64 * 64 + 64 + 2 * 64 + 2)
+
+/* Creates a model on `device` with parameters initialised from `seed`
+ * (or copied from `params` when not NULL). */
+int vine_mlp_create(int32_t device, uint64_t seed, const float *params, vine_mlp **out);
+void vine_mlp_destroy(vine_mlp *m);
+int vine_mlp_get_params(const vine_mlp *m, float *params);
+int vine_mlp_set_params(vine_mlp *m, const float *params);
+/* y[n x 2] = MLP(x[n x 16]) on the GPU (host buffers). */
+int vine_mlp_forward(const vine_mlp *m, int32_t n, const float *x, float *y);
+/* Mean squared error over n rows and its gradient w.r.t. every parameter,
+ * computed by the GPU forward + backward kernels (host buffers). */
+int vine_mlp_loss_grad(const vine_mlp *m, int32_t n, const float *x, const float *y_target,
+                       float *loss, float *grad);
+/* `epochs` passes of mini-batch Adam over (x, y_target) on the GPU; returns
+ * the final mean loss.  Mini-batches are drawn in a seeded order. */
+int vine_mlp_train(vine_mlp *m, int32_t n, const float *x, const float *y_target,
+                   int32_t epochs, int32_t batch, float lr, uint64_t seed, float *final_loss);
+
+/* Scheduler traces recorded by the last vine_solve on `g` with cfg.trace=1:
+ * one row per processed bucket.  Each row has VINE_TRACE_COLS floats:
+ * [0..15] the 16 scheduler features, [16] query index, [17] bucket width
+ * used, [18] labels expanded in the bucket, [19] rounds in the bucket. */
+#define VINE_TRACE_COLS 20
+int vine_trace_fetch(vine_graph *g, int64_t *rows, float *buf, int64_t capacity);
+
+/* --------------------------------------------------------------- autotune */
+
+/* Times candidate (block_threads, table_log2, bucket_width, split_threshold)
+ * settings of the batch engine on the given sample of queries and writes the
+ * fastest into *best (other fields copied from *base).  `cache_path` (may be
+ * NULL) stores / reuses results keyed by a fingerprint of the graph. */
+int vine_autotune(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst,
+                  const float *budget, const vine_config *base, const char *cache_path,
+                  vine_config *best);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VINE_H_ */

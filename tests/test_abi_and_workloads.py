@@ -1,0 +1,137 @@
+"""CPU tests of the boundary: the C-ABI library loads and exports every
+function the headers declare; generators are deterministic and produce the
+advertised shapes; host-side argument checking (no device needed)."""
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(vine_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_function():
+    import ctypes
+    lib = ctypes.CDLL(str(ROOT / "vine_b200" / "libvine.so"))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+    assert len(declared_functions()) >= 25
+
+
+def test_binding_covers_every_declared_function():
+    from vine_b200 import _lib
+    assert set(declared_functions()) <= set(_lib.SIGNATURES)
+
+
+def test_library_is_built_for_sm100a():
+    import subprocess
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf",
+                          str(ROOT / "vine_b200" / "libvine.so")],
+                         capture_output=True, text=True).stdout
+    assert "sm_100a" in out
+
+
+def test_config_defaults_and_names():
+    import vine_b200 as v
+    c = v.Config(engine="plain", mode="pareto", policy="ar", bucket_width=50.0)
+    d = v.config_dict(c)
+    assert d["engine"] == 1 and d["mode"] == 1 and d["policy"] == 1
+    assert d["bucket_width"] == 50.0 and d["block_threads"] == 256
+    with pytest.raises(TypeError):
+        v.Config(not_a_field=1)
+
+
+def test_grid_workload_shape_and_determinism():
+    import vine_b200 as v
+    a = v.Workload.generate(1)
+    b = v.Workload.generate(1)
+    assert a.n == 10000 and a.m == 39600 and a.nq == 16
+    for k in ("row_ptr", "col", "len", "delay", "src", "dst", "budget"):
+        assert np.array_equal(getattr(a, k), getattr(b, k))
+    assert a.len.min() >= 1 and a.len.max() <= 100 and np.all(a.len == np.round(a.len))
+    assert np.all(a.src != a.dst)
+
+
+def test_road_workload_shape():
+    import vine_b200 as v
+    w = v.Workload.generate(2, rows=50, cols=60, m_target=8400, n_pairs=4)
+    assert w.n == 3000
+    assert abs(w.m - 8400) < 600
+    # symmetric arcs with equal length both ways
+    src = np.repeat(np.arange(w.n), np.diff(w.row_ptr))
+    fwd = {(int(u), int(x)): l for u, x, l in zip(src, w.col, w.len)}
+    assert all(fwd[(x, u)] == l for (u, x), l in fwd.items())
+    assert w.nq == 12 and set(np.round(w.alpha.astype(float), 2).tolist()) == {0.2, 0.5, 0.8}
+    assert np.all(w.budget >= 0)
+
+
+def test_chunglu_and_batch_workloads():
+    import vine_b200 as v
+    w = v.Workload.generate(4, n=3000, m_target=40000, n_pairs=8)
+    deg = np.diff(w.row_ptr)
+    assert deg.max() > 20 * max(1, np.median(deg))  # heavy-tailed
+    assert w.nq == 8
+    b = v.Workload.generate(5, rows=30, cols=30, m_target=2500, n_pairs=20, hop_hi=40)
+    assert b.nq == 20 and np.all((b.alpha >= 0.1) & (b.alpha < 0.9))
+
+
+def test_budget_rule_matches_dijkstra(oracle_mod):
+    import vine_b200 as v
+    w = v.Workload.generate(2, rows=20, cols=25, m_target=1400, n_pairs=5)
+    g = oracle_mod.CsrGraph(w.row_ptr, w.col, w.len, w.delay)
+    for q in range(w.nq):
+        dmin, _, _ = oracle_mod.dijkstra(g, int(w.src[q]), "delay")
+        _, dlen, _ = oracle_mod.dijkstra(g, int(w.src[q]), "len")
+        t = int(w.dst[q])
+        want = np.floor(dmin[t] + np.float32(w.alpha[q]) * (dlen[t] - dmin[t]))
+        assert abs(float(w.budget[q]) - float(want)) <= 1.0
+
+
+def test_mtx_loader_on_reference_fixture():
+    import vine_b200 as v
+    path = Path("/root/reference/inputs/tech-routers-rf.mtx.txt")
+    if not path.exists():
+        pytest.skip("reference inputs not present")
+    w = v.Workload.load_mtx(str(path), n_pairs=3)
+    assert w.n == 2113 and w.m == 2 * 6632 and w.nq == 3
+
+
+def test_cola_loader_roundtrip(tmp_path):
+    import vine_b200 as v
+    g = tmp_path / "g.graph"
+    g.write_text("3\n0: 1 5 2 2 20 1 -1\n1: 2 7 3 -1\n2: -1\n")
+    q = tmp_path / "q.txt"
+    q.write_text("0 2 1 1 100\n0 2 1 1 4\n")
+    w = v.Workload.load_cola(str(g), str(q))
+    assert w.n == 3 and w.m == 3 and w.nq == 2
+    assert w.budget.tolist() == [100.0, 4.0]
+    assert w.col.tolist() == [1, 2, 2] and w.len.tolist() == [5, 20, 7]
+
+
+def test_loader_errors_are_status_codes(tmp_path):
+    import vine_b200 as v
+    with pytest.raises(v.VineError) as e:
+        v.Workload.load_mtx(str(tmp_path / "missing.mtx"))
+    assert e.value.status == v._lib.VINE_ERR_IO
+
+
+def test_graph_validation_without_device():
+    import vine_b200 as v
+    # a malformed graph is rejected before any device work
+    g = v.Graph([0, 2, 1], [1, 0], [1, 1], [1, 1])
+    with pytest.raises(v.VineError) as e:
+        g.make_gpu_graph()
+    assert e.value.status == v._lib.VINE_ERR_INVALID
+    g = v.Graph([0, 1, 1], [1], [-1.0], [1])
+    with pytest.raises(v.VineError):
+        g.make_gpu_graph()

@@ -1,0 +1,94 @@
+"""GPU parity: the engine (through the C ABI) against the reference's results.
+
+Golden values come from the reference's own RUN_CSPP_CPU (tests/golden);
+costs and delays must match bit-exactly, returned paths must exist, respect
+the budget and re-add to the reported cost and delay, and in Pareto mode the
+sink Pareto set must equal the reference's final sink store."""
+import numpy as np
+import pytest
+
+from golden_util import FIXTURES, check_result, csr_digest, load_fixture
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = {
+    "batch_fixed": dict(engine="batch", policy="fixed"),
+    "batch_ar": dict(engine="batch", policy="ar"),
+    "batch_small_table": dict(engine="batch", table_log2=6, spill_log2=12, split_threshold=64),
+    "batch_wide": dict(engine="batch", bucket_width=100000.0),
+    "batch_narrow": dict(engine="batch", bucket_width=1.0, block_threads=128),
+    "batch_bounds": dict(engine="batch", use_bounds=1),
+    "plain": dict(engine="plain"),
+    "plain_bounds": dict(engine="plain", use_bounds=1),
+}
+
+
+@pytest.fixture(scope="module")
+def graphs():
+    import vine_b200 as v
+    cache = {}
+
+    def get(name):
+        if name not in cache:
+            fx = load_fixture(name)
+            assert csr_digest(fx["row_ptr"], fx["col"], fx["len"], fx["delay"]) == fx["digest"]
+            cache[name] = (fx, v.Graph(fx["row_ptr"], fx["col"], fx["len"], fx["delay"]))
+        return cache[name]
+    return get
+
+
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+@pytest.mark.parametrize("name", FIXTURES)
+def test_optimal_matches_reference(graphs, name, cfg):
+    import vine_b200 as v
+    fx, g = graphs(name)
+    res = v.solve(g, fx["src"], fx["dst"], fx["budget"], v.Config(**CONFIGS[cfg]))
+    for q, expect in enumerate(fx["queries"]):
+        check_result(fx, res, q, expect)
+
+
+@pytest.mark.parametrize("engine", ["batch", "plain"])
+@pytest.mark.parametrize("name", [f for f in FIXTURES if f != "road_batch_small"])
+def test_pareto_set_matches_reference(graphs, name, engine):
+    import vine_b200 as v
+    fx, g = graphs(name)
+    res = v.solve(g, fx["src"], fx["dst"], fx["budget"], v.Config(engine=engine, mode="pareto"),
+                  pareto_stride=1024)
+    for q, expect in enumerate(fx["queries"]):
+        check_result(fx, res, q, expect)
+        want = np.array(expect["pareto"], np.float32).reshape(-1, 2)
+        got = res.pareto(q)
+        assert res.pareto_n[q] == want.shape[0], f"q{q}: {res.pareto_n[q]} vs {want.shape[0]}"
+        assert np.array_equal(got, want), f"q{q}: Pareto sets differ"
+
+
+def test_repeat_calls_are_identical(graphs):
+    import vine_b200 as v
+    fx, g = graphs("grid")
+    cfg = v.Config()
+    a = v.solve(g, fx["src"], fx["dst"], fx["budget"], cfg)
+    b = v.solve(g, fx["src"], fx["dst"], fx["budget"], cfg)
+    assert np.array_equal(a.cost, b.cost) and np.array_equal(a.delay, b.delay)
+
+
+def test_cspp_class_shim(graphs):
+    import vine_b200 as v
+    fx, g = graphs("kat3")
+    n = len(fx["queries"])
+    solver = v.cspp(g, n, [v.c_label(int(s)) for s in fx["src"]], list(map(int, fx["dst"])),
+                    [v.c_constraint(float(b)) for b in fx["budget"]])
+    assert solver.solve() == 0
+    for q, e in enumerate(fx["queries"]):
+        assert bool(solver.found_l[q]) == e["found"]
+        if e["found"]:
+            assert float(solver.cost_l[q]) == e["cost"]
+            assert solver.size_of_result_l[q] == len(solver.path_l[q]) >= 1
+
+
+def test_invalid_queries_get_status(graphs):
+    import vine_b200 as v
+    fx, g = graphs("kat3")
+    res = v.solve(g, [0, 7, 0], [2, 1, -1], [100, 5, 5], raise_on_error=False)
+    assert res.status[0] == 0 and res.found[0] == 1 and res.cost[0] == 12
+    assert res.status[1] == v._lib.VINE_ERR_INVALID and res.found[1] == 0
+    assert res.status[2] == v._lib.VINE_ERR_INVALID

@@ -1,0 +1,489 @@
+// C ABI of the engine: graph upload, configuration, solve entry points.
+//
+// vine_graph_create replaces Graph::adj_to_csr + Graph::make_gpu_graph
+// (include/graph.hpp:136-195): the CSR is uploaded as SoA arrays with the two
+// arc weights interleaved ({len, delay} per arc, one 8-byte load) and without
+// the reference's edge-id indirection (el_d[_eid_col_d[l]],
+// algorithm/bucket.cuh:73), plus a reverse CSR for the lower-bound searches.
+// vine_solve replaces cspp::solve -> RUN_CSPP (algorithm/cspp.hpp:48-53,
+// algorithm/cspp.cuh:69-325) and, unlike it, returns cost, delay, path and
+// status per query.
+
+#include "engine_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace vine {
+
+thread_local std::string g_last_error;
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int batch_slots(const vine_graph *g, const vine_config &c, int round_cap, int *slots);
+
+namespace {
+
+uint64_t fnv1a(uint64_t h, const void *data, size_t bytes) {
+  const unsigned char *p = static_cast<const unsigned char *>(data);
+  for (size_t i = 0; i < bytes; ++i) {
+    h ^= p[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// Device buffers for one host-buffer solve call.
+struct IoBuffers {
+  int32_t *src = nullptr, *dst = nullptr, *found = nullptr, *status = nullptr, *best = nullptr,
+          *pareto_n = nullptr;
+  float *budget = nullptr, *cost = nullptr, *delay = nullptr, *pareto_d = nullptr,
+        *pareto_dl = nullptr;
+  int64_t *stats = nullptr, *offsets = nullptr;
+  int32_t *path = nullptr;
+  void release() {
+    cudaFree(src);
+    cudaFree(dst);
+    cudaFree(found);
+    cudaFree(status);
+    cudaFree(best);
+    cudaFree(pareto_n);
+    cudaFree(budget);
+    cudaFree(cost);
+    cudaFree(delay);
+    cudaFree(pareto_d);
+    cudaFree(pareto_dl);
+    cudaFree(stats);
+    cudaFree(offsets);
+    cudaFree(path);
+    *this = IoBuffers();
+  }
+};
+
+}  // namespace
+
+int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
+  vine_config c;
+  if (in) {
+    c = *in;
+  } else {
+    vine_config_default(&c);
+  }
+  if (c.engine != VINE_ENGINE_BATCH && c.engine != VINE_ENGINE_PLAIN)
+    return fail(VINE_ERR_INVALID, "unknown engine");
+  if (c.mode != VINE_MODE_OPTIMAL && c.mode != VINE_MODE_PARETO)
+    return fail(VINE_ERR_INVALID, "unknown mode");
+  if (c.policy < VINE_POLICY_FIXED || c.policy > VINE_POLICY_MLP)
+    return fail(VINE_ERR_INVALID, "unknown policy");
+  if (c.policy == VINE_POLICY_MLP && c.mlp == nullptr)
+    return fail(VINE_ERR_INVALID, "VINE_POLICY_MLP needs cfg.mlp");
+  if (c.use_bounds && c.mode == VINE_MODE_PARETO)
+    return fail(VINE_ERR_INVALID, "lower bounds prune the Pareto set; use VINE_MODE_OPTIMAL");
+  if (c.use_bounds && !g->integral)
+    return fail(VINE_ERR_INVALID, "lower bounds need integral weights below 2^24");
+  if (c.block_threads == 0) c.block_threads = 256;
+  if (c.block_threads < 64 || c.block_threads > 1024 || c.block_threads % 32)
+    return fail(VINE_ERR_INVALID, "block_threads must be a multiple of 32 in [64, 1024]");
+  if (c.table_log2 == 0) c.table_log2 = 11;
+  if (c.table_log2 < 6 || c.table_log2 > 13) return fail(VINE_ERR_INVALID, "table_log2 in [6, 13]");
+  if (c.spill_log2 == 0) c.spill_log2 = 16;
+  if (c.spill_log2 < 8 || c.spill_log2 > 24) return fail(VINE_ERR_INVALID, "spill_log2 in [8, 24]");
+  if (!(c.bucket_width >= 0.0f) || !std::isfinite(c.bucket_width))
+    return fail(VINE_ERR_INVALID, "bucket_width must be finite and >= 0");
+  if (c.far_capacity == 0) c.far_capacity = int64_t(1) << 20;
+  if (c.far_capacity < 1024 || c.far_capacity > (int64_t(1) << 30))
+    return fail(VINE_ERR_INVALID, "far_capacity out of range");
+  if (c.pool_labels == 0) {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    int64_t want = (int64_t)(free_b / 8 / sizeof(Label));
+    c.pool_labels = std::min<int64_t>(want, int64_t(1) << 28);
+  }
+  if (c.pool_labels < 1024 || c.pool_labels > (int64_t(1) << 31) - (int64_t(1) << 20))
+    return fail(VINE_ERR_INVALID, "pool_labels out of range");
+  int round_cap = std::min(1024, 4 * c.block_threads);
+  if (c.split_threshold < 0) return fail(VINE_ERR_INVALID, "split_threshold must be >= 0");
+  if (c.split_threshold > 0) round_cap = std::max(32, std::min(round_cap, c.split_threshold));
+  out->width0 = c.bucket_width > 0.0f ? c.bucket_width : std::max(1.0f, 4.0f * g->mean_len);
+  out->round_cap = round_cap;
+  out->slots = 0;
+  if (c.engine == VINE_ENGINE_BATCH) VINE_TRY(batch_slots(g, c, round_cap, &out->slots));
+  out->cfg = c;
+  return VINE_OK;
+}
+
+}  // namespace vine
+
+using namespace vine;
+
+extern "C" {
+
+const char *vine_last_error(void) { return g_last_error.c_str(); }
+const char *vine_version(void) { return "vine-b200 0.1 (sm_100a)"; }
+
+void vine_config_default(vine_config *cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->engine = VINE_ENGINE_BATCH;
+  cfg->mode = VINE_MODE_OPTIMAL;
+  cfg->policy = VINE_POLICY_FIXED;
+  cfg->use_bounds = 0;
+  cfg->block_threads = 256;
+  cfg->table_log2 = 11;
+  cfg->spill_log2 = 16;
+  cfg->use_cuda_graph = 0;
+  cfg->order_queries = 1;
+}
+
+int vine_graph_create(int32_t device, int32_t n, int64_t m, const int64_t *row_ptr,
+                      const int32_t *col, const float *len, const float *delay, vine_graph **out) {
+  if (!out) return fail(VINE_ERR_INVALID, "null output handle");
+  *out = nullptr;
+  if (n < 1 || m < 0 || !row_ptr || (m > 0 && (!col || !len || !delay)))
+    return fail(VINE_ERR_INVALID, "bad graph arrays");
+  if (m >= (int64_t(1) << 31)) return fail(VINE_ERR_INVALID, "more than 2^31-1 arcs");
+  if (row_ptr[0] != 0 || row_ptr[n] != m) return fail(VINE_ERR_INVALID, "row_ptr must run 0..m");
+  for (int32_t u = 0; u < n; ++u)
+    if (row_ptr[u + 1] < row_ptr[u]) return fail(VINE_ERR_INVALID, "row_ptr not monotone");
+  bool integral = true;
+  double sum_len = 0.0;
+  for (int64_t j = 0; j < m; ++j) {
+    if (col[j] < 0 || col[j] >= n) return fail(VINE_ERR_INVALID, "arc head out of range");
+    if (!(len[j] >= 0.0f) || !(delay[j] >= 0.0f) || !std::isfinite(len[j]) ||
+        !std::isfinite(delay[j]))
+      return fail(VINE_ERR_INVALID, "weights must be finite and >= 0");
+    if (len[j] != std::floor(len[j]) || delay[j] != std::floor(delay[j]) || len[j] >= 16777216.0f ||
+        delay[j] >= 16777216.0f)
+      integral = false;
+    sum_len += len[j];
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(VINE_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(VINE_ERR_INVALID, "device out of range");
+  VINE_CUDA_TRY(cudaSetDevice(device));
+
+  std::vector<int32_t> row32((size_t)n + 1);
+  for (int32_t i = 0; i <= n; ++i) row32[i] = (int32_t)row_ptr[i];
+  std::vector<float2> w((size_t)m);
+  for (int64_t j = 0; j < m; ++j) w[j] = make_float2(len[j], delay[j]);
+  // reverse CSR (in-arcs), stable by source
+  std::vector<int32_t> rrow((size_t)n + 1, 0), rcol((size_t)m);
+  std::vector<float2> rw((size_t)m);
+  for (int64_t j = 0; j < m; ++j) rrow[(size_t)col[j] + 1]++;
+  for (int32_t i = 0; i < n; ++i) rrow[i + 1] += rrow[i];
+  std::vector<int32_t> pos(rrow.begin(), rrow.end() - 1);
+  for (int32_t u = 0; u < n; ++u)
+    for (int64_t j = row_ptr[u]; j < row_ptr[u + 1]; ++j) {
+      const int32_t p = pos[col[j]]++;
+      rcol[p] = u;
+      rw[p] = w[j];
+    }
+
+  auto *g = new vine_graph();
+  g->device = device;
+  g->n = n;
+  g->m = m;
+  g->integral = integral ? 1 : 0;
+  g->mean_len = m > 0 ? (float)(sum_len / (double)m) : 1.0f;
+  uint64_t fp = 1469598103934665603ull;
+  fp = fnv1a(fp, &n, sizeof(n));
+  fp = fnv1a(fp, row32.data(), row32.size() * sizeof(int32_t));
+  fp = fnv1a(fp, col, (size_t)m * sizeof(int32_t));
+  fp = fnv1a(fp, w.data(), w.size() * sizeof(float2));
+  g->fingerprint = fp;
+  auto cleanup = [&](int st) {
+    vine_graph_destroy(g);
+    return st;
+  };
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess)
+    return cleanup(fail(VINE_ERR_CUDA, "cudaGetDeviceProperties failed"));
+  g->sm_count = prop.multiProcessorCount;
+  const size_t mb = std::max<size_t>(1, (size_t)m);
+  if (cudaMalloc(&g->row, sizeof(int32_t) * ((size_t)n + 1)) != cudaSuccess ||
+      cudaMalloc(&g->col, sizeof(int32_t) * mb) != cudaSuccess ||
+      cudaMalloc(&g->w, sizeof(float2) * mb) != cudaSuccess ||
+      cudaMalloc(&g->rrow, sizeof(int32_t) * ((size_t)n + 1)) != cudaSuccess ||
+      cudaMalloc(&g->rcol, sizeof(int32_t) * mb) != cudaSuccess ||
+      cudaMalloc(&g->rw, sizeof(float2) * mb) != cudaSuccess)
+    return cleanup(fail(VINE_ERR_CUDA, "graph allocation failed"));
+  if (cudaMemcpy(g->row, row32.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (m > 0 && cudaMemcpy(g->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice) != cudaSuccess) ||
+      (m > 0 && cudaMemcpy(g->w, w.data(), sizeof(float2) * (size_t)m, cudaMemcpyHostToDevice) != cudaSuccess) ||
+      cudaMemcpy(g->rrow, rrow.data(), sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (m > 0 && cudaMemcpy(g->rcol, rcol.data(), sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice) != cudaSuccess) ||
+      (m > 0 && cudaMemcpy(g->rw, rw.data(), sizeof(float2) * (size_t)m, cudaMemcpyHostToDevice) != cudaSuccess))
+    return cleanup(fail(VINE_ERR_CUDA, "graph upload failed"));
+  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(VINE_ERR_CUDA, "stream creation failed"));
+  *out = g;
+  return VINE_OK;
+}
+
+void vine_graph_destroy(vine_graph *g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  g->batch.release();
+  g->plain.release();
+  cudaFree(g->row);
+  cudaFree(g->col);
+  cudaFree(g->w);
+  cudaFree(g->rrow);
+  cudaFree(g->rcol);
+  cudaFree(g->rw);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+int vine_graph_info(const vine_graph *g, int32_t *n, int64_t *m, int32_t *integral) {
+  if (!g) return fail(VINE_ERR_INVALID, "null graph");
+  if (n) *n = g->n;
+  if (m) *m = g->m;
+  if (integral) *integral = g->integral;
+  return VINE_OK;
+}
+
+static int run_engine(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d_src,
+                      const int32_t *d_dst, const float *d_budget, const int32_t *h_src,
+                      const int32_t *h_dst, const float *h_budget, const DeviceOutputs &o,
+                      cudaStream_t s, Label **pool) {
+  if (r.cfg.engine == VINE_ENGINE_BATCH)
+    return batch_run(g, r, nq, d_src, d_dst, d_budget, o, s, pool);
+  return plain_run(g, r, nq, h_src, h_dst, h_budget, o, s, pool);
+}
+
+int vine_solve_device(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst,
+                      const float *budget, const vine_config *cfg, vine_results *out,
+                      void *stream) {
+  if (!g || !out || nq < 0) return fail(VINE_ERR_INVALID, "bad arguments");
+  if (nq == 0) return VINE_OK;
+  if (!src || !dst || !budget || !out->cost || !out->delay || !out->found || !out->status)
+    return fail(VINE_ERR_INVALID, "missing input/output buffers");
+  std::lock_guard<std::mutex> lk(g->mu);
+  VINE_CUDA_TRY(cudaSetDevice(g->device));
+  Resolved r;
+  VINE_TRY(resolve_config(g, cfg, &r));
+  if (r.cfg.engine != VINE_ENGINE_BATCH)
+    return fail(VINE_ERR_INVALID, "vine_solve_device runs the batch engine only");
+  cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+  DeviceOutputs o;
+  o.cost = out->cost;
+  o.delay = out->delay;
+  o.found = out->found;
+  o.status = out->status;
+  o.stats = out->stats;
+  o.pareto_d = out->pareto_d;
+  o.pareto_delay = out->pareto_delay;
+  o.pareto_n = out->pareto_n;
+  o.pareto_stride = out->pareto_d ? out->pareto_stride : 0;
+  Label *pool = nullptr;
+  VINE_TRY(run_engine(g, r, nq, src, dst, budget, nullptr, nullptr, nullptr, o, s, &pool));
+  if (out->path_offsets && out->path) {
+    VINE_TRY(path_lengths(pool, nq, g->batch.best_idx, out->path_offsets, s));
+    // the caller guarantees path_capacity; the writer stays inside offsets
+    VINE_TRY(path_write(pool, nq, g->batch.best_idx, out->path_offsets, out->path, s));
+  }
+  return VINE_OK;
+}
+
+int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst,
+               const float *budget, const vine_config *cfg, vine_results *out) {
+  if (!g || !out || nq < 0) return fail(VINE_ERR_INVALID, "bad arguments");
+  if (nq == 0) {
+    if (out->path_offsets) out->path_offsets[0] = 0;
+    return VINE_OK;
+  }
+  if (!src || !dst || !budget || !out->cost || !out->delay || !out->found)
+    return fail(VINE_ERR_INVALID, "missing input/output buffers");
+  std::lock_guard<std::mutex> lk(g->mu);
+  VINE_CUDA_TRY(cudaSetDevice(g->device));
+  Resolved r;
+  VINE_TRY(resolve_config(g, cfg, &r));
+  cudaStream_t s = g->stream;
+  const bool want_pareto = out->pareto_d && out->pareto_delay && out->pareto_n && out->pareto_stride > 0;
+  const bool want_paths = out->path_offsets != nullptr;
+
+  std::vector<int32_t> status((size_t)nq, VINE_OK);
+  std::vector<int32_t> todo((size_t)nq);
+  for (int32_t i = 0; i < nq; ++i) todo[i] = i;
+  int attempt = 0;
+  std::vector<int64_t> all_len((size_t)nq, 0);
+  std::vector<std::vector<int32_t>> all_paths(want_paths ? (size_t)nq : 0);
+  int rc = VINE_OK;
+  while (!todo.empty()) {
+    const int32_t k = (int32_t)todo.size();
+    std::vector<int32_t> hs(k), hd(k);
+    std::vector<float> hb(k);
+    for (int32_t i = 0; i < k; ++i) {
+      hs[i] = src[todo[i]];
+      hd[i] = dst[todo[i]];
+      hb[i] = budget[todo[i]];
+    }
+    IoBuffers io;
+    auto bail = [&](int st) {
+      cudaStreamSynchronize(s);
+      io.release();
+      return st;
+    };
+    const size_t stride = want_pareto ? (size_t)out->pareto_stride : 0;
+    if (cudaMalloc(&io.src, sizeof(int32_t) * k) != cudaSuccess ||
+        cudaMalloc(&io.dst, sizeof(int32_t) * k) != cudaSuccess ||
+        cudaMalloc(&io.budget, sizeof(float) * k) != cudaSuccess ||
+        cudaMalloc(&io.cost, sizeof(float) * k) != cudaSuccess ||
+        cudaMalloc(&io.delay, sizeof(float) * k) != cudaSuccess ||
+        cudaMalloc(&io.found, sizeof(int32_t) * k) != cudaSuccess ||
+        cudaMalloc(&io.status, sizeof(int32_t) * k) != cudaSuccess ||
+        cudaMalloc(&io.best, sizeof(int32_t) * k) != cudaSuccess ||
+        cudaMalloc(&io.offsets, sizeof(int64_t) * (k + 1)) != cudaSuccess ||
+        (out->stats && cudaMalloc(&io.stats, sizeof(int64_t) * VINE_STAT_COUNT * k) != cudaSuccess) ||
+        (want_pareto && (cudaMalloc(&io.pareto_d, sizeof(float) * stride * k) != cudaSuccess ||
+                         cudaMalloc(&io.pareto_dl, sizeof(float) * stride * k) != cudaSuccess ||
+                         cudaMalloc(&io.pareto_n, sizeof(int32_t) * k) != cudaSuccess)))
+      return bail(fail(VINE_ERR_CUDA, "result allocation failed"));
+    if (cudaMemcpyAsync(io.src, hs.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(io.dst, hd.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(io.budget, hb.data(), sizeof(float) * k, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return bail(fail(VINE_ERR_CUDA, "input upload failed"));
+    DeviceOutputs o;
+    o.cost = io.cost;
+    o.delay = io.delay;
+    o.found = io.found;
+    o.status = io.status;
+    o.stats = io.stats;
+    o.pareto_d = io.pareto_d;
+    o.pareto_delay = io.pareto_dl;
+    o.pareto_n = io.pareto_n;
+    o.pareto_stride = (int32_t)stride;
+    o.best_idx = io.best;
+    Label *pool = nullptr;
+    int st = run_engine(g, r, k, io.src, io.dst, io.budget, hs.data(), hd.data(), hb.data(), o, s, &pool);
+    if (st != VINE_OK) return bail(st);
+    std::vector<int64_t> off;
+    std::vector<int32_t> path;
+    if (want_paths) {
+      if ((st = path_lengths(pool, k, io.best, io.offsets, s)) != VINE_OK) return bail(st);
+      off.resize((size_t)k + 1);
+      if (cudaMemcpyAsync(off.data(), io.offsets, sizeof(int64_t) * (k + 1), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        return bail(fail(VINE_ERR_CUDA, std::string("engine failed: ") + cudaGetErrorString(cudaGetLastError())));
+      if (off[k] > 0) {
+        if (cudaMalloc(&io.path, sizeof(int32_t) * (size_t)off[k]) != cudaSuccess)
+          return bail(fail(VINE_ERR_CUDA, "path allocation failed"));
+        if ((st = path_write(pool, k, io.best, io.offsets, io.path, s)) != VINE_OK) return bail(st);
+        path.resize((size_t)off[k]);
+        if (cudaMemcpyAsync(path.data(), io.path, sizeof(int32_t) * (size_t)off[k], cudaMemcpyDeviceToHost, s) != cudaSuccess)
+          return bail(fail(VINE_ERR_CUDA, "path download failed"));
+      }
+    }
+    std::vector<float> hc(k), hdl(k), pd, pl;
+    std::vector<int32_t> hf(k), hst(k), pn;
+    std::vector<int64_t> hstats;
+    if (cudaMemcpyAsync(hc.data(), io.cost, sizeof(float) * k, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(hdl.data(), io.delay, sizeof(float) * k, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(hf.data(), io.found, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(hst.data(), io.status, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      return bail(fail(VINE_ERR_CUDA, "result download failed"));
+    if (out->stats) {
+      hstats.resize((size_t)k * VINE_STAT_COUNT);
+      if (cudaMemcpyAsync(hstats.data(), io.stats, sizeof(int64_t) * hstats.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return bail(fail(VINE_ERR_CUDA, "stats download failed"));
+    }
+    if (want_pareto) {
+      pd.resize(stride * k);
+      pl.resize(stride * k);
+      pn.resize(k);
+      if (cudaMemcpyAsync(pd.data(), io.pareto_d, sizeof(float) * pd.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaMemcpyAsync(pl.data(), io.pareto_dl, sizeof(float) * pl.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaMemcpyAsync(pn.data(), io.pareto_n, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return bail(fail(VINE_ERR_CUDA, "pareto download failed"));
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess)
+      return bail(fail(VINE_ERR_CUDA, std::string("engine failed: ") + cudaGetErrorString(cudaGetLastError())));
+    if (r.cfg.trace && r.cfg.engine == VINE_ENGINE_BATCH && g->batch.trace) {
+      unsigned long long rows = 0;
+      cudaMemcpy(&rows, g->batch.counters + 3, sizeof(rows), cudaMemcpyDeviceToHost);
+      rows = std::min<unsigned long long>(rows, (unsigned long long)g->batch.trace_cap);
+      g->last_trace.resize((size_t)rows * VINE_TRACE_COLS);
+      if (rows)
+        cudaMemcpy(g->last_trace.data(), g->batch.trace, sizeof(float) * g->last_trace.size(), cudaMemcpyDeviceToHost);
+      // trace rows carry the engine's local query index; map back
+      for (size_t i = 0; i < (size_t)rows; ++i) {
+        float &qq = g->last_trace[i * VINE_TRACE_COLS + 16];
+        const int32_t li = (int32_t)qq;
+        if (li >= 0 && li < k) qq = (float)todo[li];
+      }
+    }
+    io.release();
+
+    std::vector<int32_t> retry;
+    for (int32_t i = 0; i < k; ++i) {
+      const int32_t q = todo[i];
+      out->cost[q] = hc[i];
+      out->delay[q] = hdl[i];
+      out->found[q] = hf[i];
+      status[q] = hst[i];
+      if (out->stats)
+        std::memcpy(out->stats + (size_t)q * VINE_STAT_COUNT, hstats.data() + (size_t)i * VINE_STAT_COUNT,
+                    sizeof(int64_t) * VINE_STAT_COUNT);
+      if (want_pareto) {
+        out->pareto_n[q] = pn[i];
+        const int32_t cnt = std::min<int32_t>(pn[i], out->pareto_stride);
+        std::memcpy(out->pareto_d + (size_t)q * stride, pd.data() + (size_t)i * stride, sizeof(float) * cnt);
+        std::memcpy(out->pareto_delay + (size_t)q * stride, pl.data() + (size_t)i * stride, sizeof(float) * cnt);
+      }
+      if (want_paths) {
+        all_len[q] = off[i + 1] - off[i];
+        all_paths[q].assign(path.begin() + off[i], path.begin() + off[i + 1]);
+      }
+      if (hst[i] == VINE_ERR_CAPACITY) retry.push_back(q);
+    }
+    if (retry.empty() || attempt >= 1) break;
+    // one retry with roomier per-worker structures for the overflowing queries
+    ++attempt;
+    r.cfg.far_capacity = std::min<int64_t>(r.cfg.far_capacity * 8, int64_t(1) << 26);
+    r.cfg.pool_labels = std::min<int64_t>(r.cfg.pool_labels * 4, (int64_t(1) << 31) - (int64_t(1) << 20));
+    r.cfg.spill_log2 = std::min(r.cfg.spill_log2 + 3, 22);
+    r.cfg.ctas_per_sm = 1;
+    r.cfg.trace = 0;
+    VINE_TRY(resolve_config(g, &r.cfg, &r));
+    todo = retry;
+  }
+  for (int32_t q = 0; q < nq; ++q) {
+    if (out->status) out->status[q] = status[q];
+    if (status[q] != VINE_OK && rc == VINE_OK) rc = status[q];
+  }
+  if (want_paths) {
+    int64_t run = 0;
+    for (int32_t q = 0; q < nq; ++q) {
+      out->path_offsets[q] = run;
+      run += all_len[q];
+    }
+    out->path_offsets[nq] = run;
+    if (run > out->path_capacity || out->path == nullptr) {
+      if (rc == VINE_OK) rc = fail(VINE_ERR_CAPACITY, "path buffer too small (need " + std::to_string(run) + ")");
+    } else {
+      for (int32_t q = 0; q < nq; ++q)
+        std::memcpy(out->path + out->path_offsets[q], all_paths[q].data(), sizeof(int32_t) * all_len[q]);
+    }
+  }
+  if (rc != VINE_OK && rc != VINE_ERR_CAPACITY) set_error("query failed with status " + std::to_string(rc));
+  if (rc == VINE_ERR_CAPACITY && g_last_error.empty()) set_error("a query exceeded engine capacity");
+  return rc;
+}
+
+int vine_trace_fetch(vine_graph *g, int64_t *rows, float *buf, int64_t capacity) {
+  if (!g || !rows) return fail(VINE_ERR_INVALID, "bad arguments");
+  const int64_t n = (int64_t)(g->last_trace.size() / VINE_TRACE_COLS);
+  *rows = n;
+  if (buf) {
+    const int64_t c = std::min(n, capacity);
+    std::memcpy(buf, g->last_trace.data(), sizeof(float) * (size_t)c * VINE_TRACE_COLS);
+  }
+  return VINE_OK;
+}
+
+}  // extern "C"

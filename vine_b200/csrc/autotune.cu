@@ -1,0 +1,162 @@
+// Autotuner for the batch engine: picks block shape (threads per query
+// worker), bucket-table size and bucket granularity (width and split
+// threshold) by timing candidates on a sample of queries with CUDA events.
+// The reference fixes these at compile time (BLOCK_SIZE, TABLE_SIZE, VSIZE,
+// algorithm/bucket.cuh:9-13; SearchSpace, algorithm/dominance.cuh:11) and
+// sizes its split from free memory (algorithm/cspp.cuh:43-47, 136-138).
+// Results are cached in a text file keyed by the graph fingerprint and the
+// search mode, so a graph is tuned once.
+
+#include "engine_host.h"
+
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+using namespace vine;
+
+namespace {
+
+struct Candidate {
+  int block_threads, table_log2, split;
+  float width_mult;
+};
+
+std::string cache_key(const vine_graph *g, const vine_config &c) {
+  std::ostringstream ss;
+  ss << std::hex << g->fingerprint << std::dec << " m" << c.mode << " b" << c.use_bounds << " p"
+     << c.policy;
+  return ss.str();
+}
+
+bool cache_lookup(const char *path, const std::string &key, Candidate *out) {
+  if (!path) return false;
+  std::ifstream in(path);
+  std::string line;
+  while (std::getline(in, line)) {
+    if (line.compare(0, key.size(), key) != 0 || line.size() <= key.size() || line[key.size()] != '|')
+      continue;
+    Candidate c;
+    if (std::sscanf(line.c_str() + key.size() + 1, "%d %d %d %f", &c.block_threads, &c.table_log2,
+                    &c.split, &c.width_mult) == 4) {
+      *out = c;
+      return true;
+    }
+  }
+  return false;
+}
+
+void cache_store(const char *path, const std::string &key, const Candidate &c) {
+  if (!path) return;
+  std::ofstream out(path, std::ios::app);
+  out << key << '|' << c.block_threads << ' ' << c.table_log2 << ' ' << c.split << ' '
+      << c.width_mult << '\n';
+}
+
+void apply(const Candidate &k, const vine_graph *g, vine_config *c) {
+  c->block_threads = k.block_threads;
+  c->table_log2 = k.table_log2;
+  c->split_threshold = k.split;
+  c->bucket_width = k.width_mult * g->mean_len;
+}
+
+}  // namespace
+
+extern "C" int vine_autotune(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst,
+                             const float *budget, const vine_config *base,
+                             const char *cache_path, vine_config *best) {
+  if (!g || nq <= 0 || !src || !dst || !budget || !best)
+    return fail(VINE_ERR_INVALID, "bad arguments");
+  vine_config b0;
+  if (base) b0 = *base;
+  else vine_config_default(&b0);
+  b0.engine = VINE_ENGINE_BATCH;
+  b0.trace = 0;
+  const std::string key = cache_key(g, b0);
+  Candidate hit;
+  if (cache_lookup(cache_path, key, &hit)) {
+    *best = b0;
+    apply(hit, g, best);
+    return VINE_OK;
+  }
+  VINE_CUDA_TRY(cudaSetDevice(g->device));
+  int32_t *d_src = nullptr, *d_dst = nullptr, *d_found = nullptr, *d_status = nullptr;
+  float *d_budget = nullptr, *d_cost = nullptr, *d_delay = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(d_src);
+    cudaFree(d_dst);
+    cudaFree(d_found);
+    cudaFree(d_status);
+    cudaFree(d_budget);
+    cudaFree(d_cost);
+    cudaFree(d_delay);
+  };
+  if (cudaMalloc(&d_src, 4 * (size_t)nq) != cudaSuccess || cudaMalloc(&d_dst, 4 * (size_t)nq) != cudaSuccess ||
+      cudaMalloc(&d_found, 4 * (size_t)nq) != cudaSuccess || cudaMalloc(&d_status, 4 * (size_t)nq) != cudaSuccess ||
+      cudaMalloc(&d_budget, 4 * (size_t)nq) != cudaSuccess || cudaMalloc(&d_cost, 4 * (size_t)nq) != cudaSuccess ||
+      cudaMalloc(&d_delay, 4 * (size_t)nq) != cudaSuccess) {
+    cleanup();
+    return fail(VINE_ERR_CUDA, "autotune allocation failed");
+  }
+  cudaMemcpy(d_src, src, 4 * (size_t)nq, cudaMemcpyHostToDevice);
+  cudaMemcpy(d_dst, dst, 4 * (size_t)nq, cudaMemcpyHostToDevice);
+  cudaMemcpy(d_budget, budget, 4 * (size_t)nq, cudaMemcpyHostToDevice);
+  std::vector<Candidate> cands;
+  for (int bt : {128, 256, 512})
+    for (int tl : {10, 11, 12})
+      for (float wm : {1.0f, 2.0f, 4.0f, 8.0f}) cands.push_back({bt, tl, 0, wm});
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best_ms = 1e30f;
+  Candidate best_c = cands[0];
+  int rc = VINE_OK;
+  for (const Candidate &k : cands) {
+    vine_config c = b0;
+    apply(k, g, &c);
+    Resolved r;
+    if (resolve_config(g, &c, &r) != VINE_OK) continue;  // does not fit: skip
+    DeviceOutputs o;
+    o.cost = d_cost;
+    o.delay = d_delay;
+    o.found = d_found;
+    o.status = d_status;
+    float ms_total = 0.0f;
+    bool ok = true;
+    for (int rep = 0; rep < 2 && ok; ++rep) {
+      cudaEventRecord(e0, g->stream);
+      if (batch_run(g, r, nq, d_src, d_dst, d_budget, o, g->stream, nullptr) != VINE_OK) ok = false;
+      cudaEventRecord(e1, g->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = fail(VINE_ERR_CUDA, "autotune run failed");
+        ok = false;
+        break;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep == 1) ms_total = ms;  // first run warms the workspace
+    }
+    if (rc != VINE_OK) break;
+    if (!ok) continue;
+    std::vector<int32_t> st((size_t)nq);
+    cudaMemcpy(st.data(), d_status, 4 * (size_t)nq, cudaMemcpyDeviceToHost);
+    bool all_ok = true;
+    for (int32_t v : st) all_ok = all_ok && v == VINE_OK;
+    if (all_ok && ms_total < best_ms) {
+      best_ms = ms_total;
+      best_c = k;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cleanup();
+  if (rc != VINE_OK) return rc;
+  if (best_ms >= 1e30f) return fail(VINE_ERR_CAPACITY, "no autotune candidate solved the sample");
+  *best = b0;
+  apply(best_c, g, best);
+  cache_store(cache_path, key, best_c);
+  return VINE_OK;
+}

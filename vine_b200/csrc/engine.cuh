@@ -1,0 +1,428 @@
+// Device-side building blocks of the exact CSP engine (sm_100a).
+//
+// Search order.  Labels are processed in buckets of a key f = d + h(v), where
+// h is a consistent lower bound on the remaining cost (0 without bounds).
+// A bucket is the key range [lo, hi); it is expanded in synchronous rounds
+// until no label with key in range remains.  Children of a label never have a
+// smaller key (consistency), so once a bucket is finished every later label
+// at vertex v has a larger d than every label of the bucket at v.  Hence the
+// labels of finished buckets at v can be summarised by one number, the
+// smallest delay among them ("settled delay", VState::sdel): a candidate is
+// dominated by a settled label iff its delay is >= sdel.  Inside the open
+// bucket, labels are compared exactly against each other in a per-vertex
+// bucket table (shared-memory hash table, spill to HBM).  The reference's
+// dominance (include/label.hpp:234-236) and constraint
+// (include/constraint.hpp:99-101) are applied unchanged; only the order of
+// work differs, so the surviving sink labels are the same.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vine {
+
+constexpr int32_t kEmpty = -1;
+constexpr uint32_t kDeadBit = 0x80000000u;
+constexpr int kSpinLimit = 1 << 22;  // bounded lock spins before giving up
+
+// One accepted label in the arena.  vid's top bit marks a label killed by a
+// dominating label of the same bucket.  parent is the arena index of the label
+// it was expanded from (-1 for the source).
+struct Label {
+  int32_t vid;
+  float d;
+  float dl;
+  int32_t parent;
+};
+
+// Per (worker, vertex) state, lazily reset through the query epoch.
+struct VState {
+  uint32_t epoch;
+  float sdel;  // smallest delay of labels at v in finished buckets
+  float hlen;  // lower bound on the remaining cost (bounds mode)
+  float hdel;  // lower bound on the remaining delay (bounds mode)
+};
+
+// Bucket-table entry.  vid == kEmpty marks a free slot; idx's top bit marks
+// a killed entry.
+struct TEntry {
+  int32_t vid;
+  float d;
+  float dl;
+  uint32_t idx;
+};
+
+struct DevGraph {
+  int32_t n;
+  int64_t m;
+  const int32_t *row;  // [n+1]
+  const int32_t *col;  // [m]
+  const float2 *w;     // [m] {len, delay}
+  const int32_t *rrow; // reverse CSR (in-arcs)
+  const int32_t *rcol;
+  const float2 *rw;
+};
+
+// ------------------------------------------------------------------ helpers
+
+__device__ __forceinline__ uint64_t pack_key(float d, float dl) {
+  // For non-negative floats the IEEE bit patterns are ordered like the
+  // values, so this 64-bit key orders labels lexicographically by (d, dl).
+  return ((uint64_t)__float_as_uint(d) << 32) | (uint64_t)__float_as_uint(dl);
+}
+__device__ __forceinline__ float key_d(uint64_t k) { return __uint_as_float((uint32_t)(k >> 32)); }
+__device__ __forceinline__ float key_dl(uint64_t k) { return __uint_as_float((uint32_t)k); }
+
+__device__ __forceinline__ bool dominates(float ad, float al, float bd, float bl) {
+  return ad <= bd && al <= bl;  // include/label.hpp:234-236
+}
+
+__device__ __forceinline__ uint32_t hash_vid(int32_t v, int log2n) {
+  return ((uint32_t)v * 2654435769u) >> (32 - log2n);
+}
+
+// Warp-aggregated increment: one atomic per group of converged lanes.
+__device__ __forceinline__ uint32_t warp_agg_inc(uint32_t *ctr) {
+  namespace cg = cooperative_groups;
+  cg::coalesced_group grp = cg::coalesced_threads();
+  uint32_t base = 0;
+  if (grp.thread_rank() == 0) base = atomicAdd(ctr, (uint32_t)grp.size());
+  base = grp.shfl(base, 0);
+  return base + (uint32_t)grp.thread_rank();
+}
+
+__device__ __forceinline__ void atomic_min_float_nonneg(float *addr, float v) {
+  // non-negative floats order like their bit patterns
+  atomicMin(reinterpret_cast<unsigned int *>(addr), __float_as_uint(v));
+}
+
+// Runs `body` while holding spin lock *l and returns true, or returns false
+// after kSpinLimit failed attempts.  The critical section and the release
+// sit inside the spin loop: a lane that took the lock finishes and releases
+// it before it can reach any reconvergence point where it might wait for a
+// lane of its own warp that is still spinning on the same lock.
+template <typename Body>
+__device__ __forceinline__ bool with_lock(int *l, Body body) {
+  for (int it = 0; it < kSpinLimit; ++it) {
+    if (atomicCAS(l, 0, 1) == 0) {
+      __threadfence_block();
+      body();
+      __threadfence_block();
+      atomicExch(l, 0);
+      return true;
+    }
+  }
+  return false;
+}
+
+// Folds one label of a finished bucket into the settled delay of v.
+__device__ __forceinline__ void settle(VState *vs, uint32_t epoch, float dl) {
+  unsigned long long *w = reinterpret_cast<unsigned long long *>(vs);
+  unsigned long long old = *reinterpret_cast<volatile unsigned long long *>(w);
+  for (;;) {
+    const uint32_t e = (uint32_t)old;
+    const float s = __uint_as_float((uint32_t)(old >> 32));
+    if (e == epoch && s <= dl) return;
+    const unsigned long long nw = ((unsigned long long)__float_as_uint(dl) << 32) | epoch;
+    const unsigned long long prev = atomicCAS(w, old, nw);
+    if (prev == old) return;
+    old = prev;
+  }
+}
+
+// ------------------------------------------------------------ block scan
+
+// Exclusive prefix sum of a[0..n) in place (shared memory), returns the total.
+// `scratch` holds >= 33 ints of shared memory.  All threads must call.
+__device__ inline int block_exclusive_scan(int *a, int n, int *scratch) {
+  const int G = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = (G + 31) >> 5;
+  const int per = (n + G - 1) / G;
+  const int beg = min(n, tid * per), end = min(n, beg + per);
+  int local = 0;
+  for (int i = beg; i < end; ++i) local += a[i];
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) scratch[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int v = lane < nwarps ? scratch[lane] : 0;
+    int vi = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, vi, o);
+      if (lane >= o) vi += y;
+    }
+    if (lane < nwarps) scratch[lane] = vi - v;  // exclusive warp offsets
+    if (lane == nwarps - 1) scratch[32] = vi;   // total
+  }
+  __syncthreads();
+  int run = scratch[warp] + incl - local;
+  for (int i = beg; i < end; ++i) {
+    int x = a[i];
+    a[i] = run;
+    run += x;
+  }
+  const int total = scratch[32];
+  __syncthreads();
+  return total;
+}
+
+// Largest i in [0, n) with off[i] <= e (off non-decreasing, off[0] = 0 <= e).
+__device__ __forceinline__ int upper_index(const int *off, int n, int e) {
+  int lo = 0, hi = n;  // invariant: off[lo] <= e, answer in [lo, hi)
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (off[mid] <= e) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// ------------------------------------------------------------ bucket table
+
+// Outcome of inserting a candidate into the bucket table.
+enum InsertResult { kInserted = 0, kDominated = 1, kFull = 2, kLockTimeout = 3 };
+
+struct BucketTable {
+  TEntry *t;         // shared-memory table
+  int log2h;         // entries = 1 << log2h
+  int probe;         // max probe window in the shared table
+  int *locks;        // striped locks (shared memory)
+  int lock_mask;
+  TEntry *s;         // HBM spill table of this worker
+  int log2s;
+  uint32_t *s_used;  // positions used in the spill table
+  uint32_t *s_count; // number of used spill positions (shared memory)
+  uint32_t s_limit;  // fail beyond this many spilled labels
+};
+
+// Checks candidate (v, d, dl) against the labels of the open bucket at v,
+// kills the ones it dominates (marking their arena labels dead) and, when it
+// is not dominated, stores it with arena index `idx_alloc()`.  Exact: all
+// operations on one vertex are serialised by that vertex's stripe lock, and
+// a candidate is only dropped when a stored label dominates it.
+constexpr uint32_t kBadIdx = 0xffffffffu;  // allocator out of arena space
+
+// Body of table_insert; the caller holds v's stripe lock.
+template <typename Alloc>
+__device__ InsertResult table_insert_locked(const BucketTable &bt, Label *pool, int32_t v,
+                                            float d, float dl, Alloc &idx_alloc,
+                                            uint32_t *out_idx, bool *spilled) {
+  const uint32_t hmask = (1u << bt.log2h) - 1u;
+  const uint32_t h0 = hash_vid(v, bt.log2h);
+  volatile TEntry *T = bt.t;
+  int free_p = -1;
+  for (int p = 0; p < bt.probe; ++p) {
+    volatile TEntry *e = &T[(h0 + p) & hmask];
+    const int32_t ev = e->vid;
+    if (ev == kEmpty) {
+      free_p = p;
+      break;
+    }
+    if (ev != v) continue;
+    const uint32_t eidx = e->idx;
+    if (eidx & kDeadBit) continue;
+    const float ed = e->d, el = e->dl;
+    if (dominates(ed, el, d, dl)) return kDominated;
+    if (dominates(d, dl, ed, el)) {
+      e->idx = eidx | kDeadBit;
+      atomicOr(reinterpret_cast<unsigned int *>(&pool[eidx].vid), kDeadBit);
+    }
+  }
+  const bool window_full = (free_p < 0);
+  const uint32_t smask = (1u << bt.log2s) - 1u;
+  if (window_full && *reinterpret_cast<volatile uint32_t *>(bt.s_count) > 0) {
+    // the shared window was already full when earlier labels of v arrived:
+    // they may live in the spill table
+    volatile TEntry *S = bt.s;
+    const uint32_t g0 = hash_vid(v, bt.log2s);
+    for (uint32_t q = 0; q <= smask; ++q) {
+      volatile TEntry *e = &S[(g0 + q) & smask];
+      const int32_t ev = e->vid;
+      if (ev == kEmpty) break;
+      if (ev != v) continue;
+      const uint32_t eidx = e->idx;
+      if (eidx & kDeadBit) continue;
+      const float ed = e->d, el = e->dl;
+      if (dominates(ed, el, d, dl)) return kDominated;
+      if (dominates(d, dl, ed, el)) {
+        e->idx = eidx | kDeadBit;
+        atomicOr(reinterpret_cast<unsigned int *>(&pool[eidx].vid), kDeadBit);
+      }
+    }
+  }
+  // not dominated: claim a slot (labels of other vertices may race for it)
+  if (!window_full) {
+    for (int p = free_p; p < bt.probe; ++p) {
+      TEntry *e = &bt.t[(h0 + p) & hmask];
+      if (atomicCAS(&e->vid, kEmpty, v) == kEmpty) {
+        const uint32_t idx = idx_alloc();
+        if (idx == kBadIdx) {
+          e->idx = kDeadBit;  // keeps the probe chain intact; never expanded
+          return kFull;
+        }
+        e->d = d;
+        e->dl = dl;
+        e->idx = idx;
+        *out_idx = idx;
+        *spilled = false;
+        return kInserted;
+      }
+    }
+  }
+  // spill to the HBM table of this worker
+  const uint32_t cnt = atomicAdd(bt.s_count, 1u);
+  if (cnt >= bt.s_limit) {
+    atomicSub(bt.s_count, 1u);
+    return kFull;
+  }
+  const uint32_t g0 = hash_vid(v, bt.log2s);
+  for (uint32_t q = 0; q <= smask; ++q) {
+    const uint32_t pos = (g0 + q) & smask;
+    TEntry *e = &bt.s[pos];
+    if (atomicCAS(&e->vid, kEmpty, v) == kEmpty) {
+      bt.s_used[cnt] = pos;
+      const uint32_t idx = idx_alloc();
+      if (idx == kBadIdx) {
+        e->idx = kDeadBit;
+        return kFull;
+      }
+      e->d = d;
+      e->dl = dl;
+      e->idx = idx;
+      *out_idx = idx;
+      *spilled = true;
+      return kInserted;
+    }
+  }
+  return kFull;
+}
+
+// Checks candidate (v, d, dl) against the labels of the open bucket at v,
+// kills the ones it dominates (marking their arena labels dead) and, when it
+// is not dominated, stores it with arena index `idx_alloc()` (which also
+// writes the arena label, so a kill can never be overwritten).  Exact: all
+// operations on one vertex are serialised by that vertex's stripe lock, and
+// a candidate is only dropped when a stored label dominates it.
+template <typename Alloc>
+__device__ InsertResult table_insert(const BucketTable &bt, Label *pool, int32_t v, float d,
+                                     float dl, Alloc idx_alloc, uint32_t *out_idx,
+                                     bool *spilled) {
+  int *lk = &bt.locks[(uint32_t)v & (uint32_t)bt.lock_mask];
+  InsertResult r = kLockTimeout;
+  with_lock(lk, [&]() { r = table_insert_locked(bt, pool, v, d, dl, idx_alloc, out_idx, spilled); });
+  return r;
+}
+
+// ------------------------------------------------ scheduler (AR and MLP)
+
+constexpr int kFeat = 16;
+constexpr int kHid = 64;
+constexpr int kOut = 2;
+constexpr int kMlpParams = kHid * kFeat + kHid + kHid * kHid + kHid + kOut * kHid + kOut;
+
+// Burg's maximum-entropy AR(p) fit (J. P. Burg, 1967; the recursion as given
+// in standard spectral-estimation texts) of the mean-removed series x[0..n),
+// then a one-step forecast x_hat[n].  Plays the role of the reference's
+// AR::AutoRegression / ARMaxEntropy (include/AR.cpp:6-147) as used by
+// RUN_CSPP (algorithm/cspp.cuh:263-284).  Returns false when the fit is
+// degenerate (constant series or too few points).
+constexpr int kBurgMaxN = 32;
+__host__ __device__ inline bool burg_forecast(const double *x, int n, int p, double *out) {
+  if (n <= p || p < 1 || p > 8 || n > kBurgMaxN) return false;
+  double mean = 0.0;
+  for (int i = 0; i < n; ++i) mean += x[i];
+  mean /= n;
+  double f[kBurgMaxN], b[kBurgMaxN], a[9], an[9];
+  for (int i = 0; i < n; ++i) f[i] = b[i] = x[i] - mean;
+  for (int i = 0; i <= p; ++i) a[i] = 0.0;
+  a[0] = 1.0;
+  for (int m = 1; m <= p; ++m) {
+    double num = 0.0, den = 0.0;
+    for (int k = m; k < n; ++k) {
+      num += f[k] * b[k - 1];
+      den += f[k] * f[k] + b[k - 1] * b[k - 1];
+    }
+    if (!(den > 0.0)) return false;
+    const double km = -2.0 * num / den;
+    for (int i = 0; i <= m; ++i) an[i] = a[i] + km * (m - i >= 0 ? a[m - i] : 0.0);
+    for (int i = 0; i <= m; ++i) a[i] = an[i];
+    // update prediction errors, from the end so b[k-1] is still the old value
+    for (int k = n - 1; k >= m; --k) {
+      const double fk = f[k], bk = b[k - 1];
+      f[k] = fk + km * bk;
+      b[k] = bk + km * fk;
+    }
+  }
+  double pred = 0.0;
+  for (int i = 1; i <= p; ++i) pred -= a[i] * (x[n - i] - mean);
+  *out = mean + pred;
+  return true;
+}
+
+// Scheduler features of one bucket boundary (the 16 MLP inputs).
+struct BucketStats {
+  float far_n, bucket_labels, expanded, rounds, total_expanded, buckets, width_rel,
+      dominated_frac, inc_found, inc_gap, far_gap, table_fill, spilled, mean_degree, ar_delta,
+      budget_rel;
+};
+
+__host__ __device__ inline void make_features(const BucketStats &s, float *x) {
+  x[0] = log2f(1.0f + s.far_n);
+  x[1] = log2f(1.0f + s.bucket_labels);
+  x[2] = log2f(1.0f + s.expanded);
+  x[3] = log2f(1.0f + s.rounds);
+  x[4] = log2f(1.0f + s.total_expanded);
+  x[5] = log2f(1.0f + s.buckets);
+  x[6] = s.width_rel;
+  x[7] = s.dominated_frac;
+  x[8] = s.inc_found;
+  x[9] = s.inc_gap;
+  x[10] = s.far_gap;
+  x[11] = s.table_fill;
+  x[12] = s.spilled;
+  x[13] = s.mean_degree;
+  x[14] = s.ar_delta;
+  x[15] = s.budget_rel;
+}
+
+// Forward pass of the 16-64-64-2 ReLU MLP by one warp (lanes split the 64
+// hidden units two each).  params layout: W1[64][16] b1[64] W2[64][64] b2[64]
+// W3[2][64] b3[2].  `h` is 128 floats of scratch visible to the warp.
+__device__ inline void mlp_forward_warp(const float *__restrict__ params, const float *x,
+                                        float *h, float *y) {
+  const int lane = threadIdx.x & 31;
+  const float *W1 = params, *b1 = W1 + kHid * kFeat, *W2 = b1 + kHid, *b2 = W2 + kHid * kHid,
+              *W3 = b2 + kHid, *b3 = W3 + kOut * kHid;
+  for (int j = lane; j < kHid; j += 32) {
+    float acc = b1[j];
+    for (int i = 0; i < kFeat; ++i) acc += W1[j * kFeat + i] * x[i];
+    h[j] = fmaxf(acc, 0.0f);
+  }
+  __syncwarp();
+  float h2[2];
+  for (int r = 0; r < 2; ++r) {
+    const int j = lane + 32 * r;
+    float acc = b2[j];
+    for (int i = 0; i < kHid; ++i) acc += W2[j * kHid + i] * h[i];
+    h2[r] = fmaxf(acc, 0.0f);
+  }
+  __syncwarp();
+  h[kHid + lane] = h2[0];
+  h[kHid + lane + 32] = h2[1];
+  __syncwarp();
+  if (lane < kOut) {
+    float acc = b3[lane];
+    for (int i = 0; i < kHid; ++i) acc += W3[lane * kHid + i] * h[kHid + i];
+    y[lane] = acc;
+  }
+  __syncwarp();
+}
+
+}  // namespace vine
