@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""Benchmark: exact CSP queries/s on the 264k-vertex road-like workload.
+
+Workload: 4096 queries on the seeded 264,000-vertex / 733,434-arc road-like
+graph (sink at a BFS hop distance log-uniform in [10, 2000], budget fraction
+alpha ~ U[0.1, 0.9]); synthetic data, generated by the library's seeded
+generator.  One step = one pass of the batched engine over the whole batch
+(results and paths included).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vine|reference]
+
+With N > 1 (launched by torchrun) every rank solves its own 4096-query batch
+on the same graph (queries from a rank-specific seed): weak scaling, no
+collective on the data path; only the timing uses a barrier and a max.
+
+Prints one JSON line (rank 0).  `value` is device-resident throughput (inputs
+already in HBM, CUDA events per step, L2 flushed between steps); `e2e` is the
+same metric through the public host API (vine_solve) with pinned host inputs.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "exact CSP queries/sec, batched+learned vs plain GPU, 264k-vertex road graph"
+WORKLOAD = "road264k-4096q"
+MODEL_PATH = ROOT / "vine_b200" / "models" / "scheduler_mlp.npy"
+COUNTERS_PATH = ROOT / "vine_b200" / "models" / "c5_algorithmic_work.json"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vine", choices=["vine", "reference"])
+    ap.add_argument("--nq", type=int, default=4096)
+    ap.add_argument("--policy", default="auto", choices=["auto", "fixed", "ar", "mlp"])
+    ap.add_argument("--no-baselines", action="store_true", help="skip CPU / plain-GPU legs")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(rank: int, nq: int):
+    import vine_b200 as v
+    over = {"n_pairs": nq}
+    if rank > 0:
+        over["query_seed"] = 0x5EED0000 + rank
+    return v.Workload.generate(5, **over)
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+def load_work_counts():
+    """Algorithmic work per query (oracle label setting under the engine's
+    pruning rules), precomputed by tests/golden/make_work_counts.py."""
+    p = ROOT / "tests" / "golden" / "road264k_work.json"
+    if not p.exists():
+        return None
+    return json.loads(p.read_text())
+
+
+def algorithmic_bytes(work: dict) -> float:
+    t = work["totals"]
+    forward = 20 * t["P"] + 12 * t["R"] + 8 * t["S"] + 24 * t["I"]
+    bounds = 20 * t["bound_vertices"] + 16 * t["bound_arcs"]
+    return float(forward + bounds)
+
+
+def engine_config(v, policy: str, mlp, width: float):
+    base = dict(use_bounds=1, bucket_width=width)
+    if policy == "mlp" and mlp is not None:
+        return v.Config(policy="mlp", mlp=mlp, **base)
+    if policy == "fixed":
+        return v.Config(policy="fixed", **base)
+    return v.Config(policy="ar", **base)
+
+
+def cpu_reference_sample(w, count: int = 512):
+    """Runs the reference's own CPU solver (RUN_CSPP_CPU, compiled from the
+    reference sources into oracle/_ref) with every host thread on a bounded
+    sample: the `count` queries with the smallest budgets, which the
+    exhaustive CPU search finishes in seconds (larger budgets take minutes per
+    query).  The rate is therefore an upper bound on the CPU's rate over the
+    whole workload."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    g = O.CsrGraph(w.row_ptr, w.col, w.len, w.delay)
+    ref = O.RefSolver(g)
+    threads = O.cpu_count()
+    sel = np.argsort(w.budget, kind="stable")[:count]
+    t = time.perf_counter()
+    ref.solve(w.src[sel], w.dst[sel], w.budget[sel], nthreads=threads)
+    elapsed = time.perf_counter() - t
+    ref.close()
+    return {"value": len(sel) / elapsed, "unit": "queries/s", "cores": threads, "kind": "reference",
+            "sample": f"the {len(sel)} smallest-budget queries of the {w.nq}-query batch "
+                      f"({len(sel) / w.nq:.1%}), reference RUN_CSPP_CPU, {threads} threads; "
+                      "easiest queries, so an upper bound on the CPU rate",
+            "seconds": elapsed}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import vine_b200 as v  # generator only
+    w = workload(0, args.nq)
+    res = None
+    times = []
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU "
+                          "solver built from its sources) is missing"}))
+        return
+    g = O.CsrGraph(w.row_ptr, w.col, w.len, w.delay)
+    ref = O.RefSolver(g)
+    threads = O.cpu_count()
+    order = np.argsort(w.budget, kind="stable")
+    per_step = max(threads * 4, 32)
+    for i in range(args.warmup + args.steps):
+        sel = order[(i * per_step) % len(order):][:per_step]
+        t = time.perf_counter()
+        ref.solve(w.src[sel], w.dst[sel], w.budget[sel], nthreads=threads)
+        dt = time.perf_counter() - t
+        if i >= args.warmup:
+            times.append((len(sel), dt))
+    ref.close()
+    nqs = sum(n for n, _ in times)
+    tot = sum(t for _, t in times)
+    value = nqs / tot
+    sample = (f"per step the {per_step} next-smallest-budget queries of the {w.nq}-query batch "
+              f"(easiest first), reference RUN_CSPP_CPU with {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "queries_per_step": per_step, "graph": "road 264000 V / 733434 arcs"},
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_vine(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    import vine_b200 as v
+    dev = torch.device(f"cuda:{local}")
+    w = workload(rank, args.nq)
+    nq = w.nq
+    g = v.Graph(w.row_ptr, w.col, w.len, w.delay, device=local)
+
+    policy, mlp = args.policy, None
+    if policy in ("auto", "mlp") and MODEL_PATH.exists():
+        mlp = v.MLP(device=local, params=np.load(MODEL_PATH))
+        policy = "mlp"
+    elif policy in ("auto", "mlp"):
+        policy = "ar"
+    width0 = float(0.25 * w.len.mean())
+    cfg = engine_config(v, policy, mlp, width0)
+    tuned = ROOT / "vine_b200" / "models" / "autotune_road264k.json"
+    if tuned.exists():
+        for k, val in json.loads(tuned.read_text()).items():
+            setattr(cfg, k, val)
+    cfg_graph = engine_config(v, policy, mlp, width0)
+    for k in ("block_threads", "table_log2", "bucket_width", "split_threshold"):
+        setattr(cfg_graph, k, getattr(cfg, k))
+    cfg_graph.use_cuda_graph = 1
+
+    src = torch.from_numpy(w.src).to(dev)
+    dst = torch.from_numpy(w.dst).to(dev)
+    bud = torch.from_numpy(w.budget).to(dev)
+    path_cap = nq * 4096
+    out = {"cost": torch.empty(nq, dtype=torch.float32, device=dev),
+           "delay": torch.empty(nq, dtype=torch.float32, device=dev),
+           "found": torch.empty(nq, dtype=torch.int32, device=dev),
+           "status": torch.empty(nq, dtype=torch.int32, device=dev),
+           "path_offsets": torch.empty(nq + 1, dtype=torch.int64, device=dev),
+           "path": torch.empty(path_cap, dtype=torch.int32, device=dev)}
+    out_nopath = {k: out[k] for k in ("cost", "delay", "found", "status")}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def step():
+        v.solve_device(g, src, dst, bud, out, cfg_graph, stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    status = out["status"].cpu().numpy()
+    if (status != 0).any():
+        r = v.solve(g, w.src[status != 0][:64], w.dst[status != 0][:64], w.budget[status != 0][:64],
+                    cfg, paths=False, stats=True, raise_on_error=False)
+        raise SystemExit(f"rank {rank}: {(status != 0).sum()} queries failed (status "
+                         f"{np.unique(status)}; abort sites {np.unique(r.stats[:, 8])})")
+    parity = None
+    work = load_work_counts()
+    if rank == 0 and work is not None and work.get("nq") == nq:
+        cost = out["cost"].cpu().numpy()
+        found = out["found"].cpu().numpy()
+        exp_found = np.array([q["found"] for q in work["queries"]])
+        exp_cost = np.array([q["cost"] if q["found"] else np.inf for q in work["queries"]], np.float32)
+        bad = (found.astype(bool) != exp_found) | (exp_found & (cost != exp_cost))
+        parity = {"checked": int(nq), "mismatches": int(bad.sum()),
+                  "against": "oracle label-setting costs (tests/golden/road264k_work.json)"}
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize(dev)
+    sampler.start()
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between steps, outside the timed events
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    barrier()
+    clocks = sampler.stop()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * nq * args.steps / (ms_max / 1e3)
+
+    # kernel-level timing for the roofline: the same launch without paths
+    kern = []
+    for i in range(max(2, args.steps) + 1):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        v.solve_device(g, src, dst, bud, out_nopath, cfg, stream)
+        e1.record()
+        if i > 0:
+            kern.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in kern]))
+
+    # end to end through the host API, pinned host buffers
+    hs = torch.from_numpy(w.src).pin_memory().numpy()
+    hd = torch.from_numpy(w.dst).pin_memory().numpy()
+    hb = torch.from_numpy(w.budget).pin_memory().numpy()
+    e2e_steps = max(2, min(args.steps, 3))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        r = v.solve(g, hs, hd, hb, cfg, paths=True, path_capacity=path_cap)
+    t_e2e = time.perf_counter() - t0
+    t_t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * nq * e2e_steps / float(t_t.item())
+    d2h = nq * 16 + (nq + 1) * 8 + int(r.path_offsets[-1]) * 4
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = measured_peak_hbm()
+    roof = None
+    if work is not None and work.get("nq") == nq:
+        alg = algorithmic_bytes(work)
+        achieved = alg / (kern_ms / 1e3) / 1e9
+        traffic = None
+        tp = ROOT / "profiles" / "batch_kernel_traffic.json"
+        if tp.exists():
+            traffic = json.loads(tp.read_text()).get("dram_bytes_per_launch_scaled")
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": alg, "kernel_ms": kern_ms,
+                "kernel": "batch_kernel (+ epoch/order kernels, < 0.1%)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "graph": f"road {w.n} V / {w.m} arcs", "queries": nq,
+                   "policy": policy, "bounds": "reverse delay + A* length",
+                   "block_threads": cfg.block_threads, "table_log2": cfg.table_log2,
+                   "bucket_width": cfg.bucket_width, "split_threshold": cfg.split_threshold,
+                   "cuda_graph": True, "l2": "flushed between steps (256 MiB write)"},
+        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": nq * 12,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": 6 * args.steps,
+        "clocks": clocks,
+        "roofline": roof,
+        "parity": parity,
+    }
+    if not args.no_baselines and world == 1:
+        line["cpu_baseline"] = cpu_reference_sample(w)
+        # the plain engine (whole GPU, one query at a time) on a sample
+        k = 32
+        cfg_plain = v.Config(engine="plain", policy="ar", use_bounds=1)
+        v.solve(g, w.src[:4], w.dst[:4], w.budget[:4], cfg_plain, paths=False)
+        t0 = time.perf_counter()
+        rp = v.solve(g, w.src[:k], w.dst[:k], w.budget[:k], cfg_plain, paths=False)
+        tp = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rb = v.solve(g, w.src[:k], w.dst[:k], w.budget[:k], cfg, paths=False)
+        tb = time.perf_counter() - t0
+        line["plain_gpu"] = {"value": k / tp, "unit": "queries/s", "sample": f"first {k} queries",
+                             "batched_same_sample": k / tb,
+                             "agree": bool(np.array_equal(rp.cost, rb.cost))}
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_vine(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -115,9 +115,13 @@ enum vine_stat {
   VINE_STAT_DOMINATED,    /* candidates rejected by dominance                */
   VINE_STAT_BUCKETS,      /* buckets processed                               */
   VINE_STAT_ROUNDS,       /* expansion rounds                                */
-  VINE_STAT_SPILLS,       /* labels placed in the HBM spill table            */
+  VINE_STAT_SPILLS,       /* labels stored in per-vertex HBM overflow chains */
   VINE_STAT_CYCLES,       /* device clock cycles spent on the query          */
-  VINE_STAT_COUNT = 8
+  VINE_STAT_ABORT_SITE,   /* where a failed query stopped (0 = it did not)   */
+  VINE_STAT_BOUND_ROUNDS, /* rounds of the reverse bound searches            */
+  VINE_STAT_BOUND_CYCLES, /* device clock cycles of the reverse searches     */
+  VINE_STAT_CHAIN_STEPS,  /* overflow-chain labels read by dominance tests   */
+  VINE_STAT_COUNT = 12
 };
 
 typedef struct {

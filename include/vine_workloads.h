@@ -47,6 +47,8 @@ typedef struct {
   int32_t hop_lo, hop_hi; /* sink sampled at a BFS hop distance in [lo,hi];    */
   int32_t hop_log_uniform;/* 0 = uniform random pairs when hop_hi == 0          */
   int32_t nthreads;    /* host threads for budgets / BFS (0 = all cores)       */
+  uint64_t query_seed; /* 0: queries continue the graph's random stream;       */
+                       /* else they come from their own stream with this seed */
 } vine_workload_params;
 
 /* Default parameters of the five benchmark workloads (config_id 1..5). */

@@ -29,12 +29,17 @@ def graphs():
     cache = {}
 
     def get(name):
+        # one graph alive at a time: each holds its engines' device workspaces
         if name not in cache:
+            for old in list(cache):
+                cache.pop(old)[1].close()
             fx = load_fixture(name)
             assert csr_digest(fx["row_ptr"], fx["col"], fx["len"], fx["delay"]) == fx["digest"]
             cache[name] = (fx, v.Graph(fx["row_ptr"], fx["col"], fx["len"], fx["delay"]))
         return cache[name]
-    return get
+    yield get
+    for fx, g in cache.values():
+        g.close()
 
 
 @pytest.mark.parametrize("cfg", list(CONFIGS))

@@ -32,8 +32,9 @@ STATUS_NAMES = {
 ENGINE_BATCH, ENGINE_PLAIN = 0, 1
 MODE_OPTIMAL, MODE_PARETO = 0, 1
 POLICY_FIXED, POLICY_AR, POLICY_MLP = 0, 1, 2
-STAT_NAMES = ["expanded", "relaxed", "inserted", "dominated", "buckets", "rounds", "spills", "cycles"]
-STAT_COUNT = 8
+STAT_NAMES = ["expanded", "relaxed", "inserted", "dominated", "buckets", "rounds", "spills",
+              "cycles", "abort_site", "bound_rounds", "bound_cycles", "chain_steps"]
+STAT_COUNT = 12
 MLP_IN, MLP_HIDDEN, MLP_OUT = 16, 64, 2
 MLP_PARAMS = 64 * 16 + 64 + 64 * 64 + 64 + 2 * 64 + 2
 TRACE_COLS = 20
@@ -66,6 +67,7 @@ class vine_workload_params(C.Structure):
         ("n_pairs", C.c_int32), ("n_alpha", C.c_int32), ("alpha", C.c_float * 4),
         ("alpha_lo", C.c_float), ("alpha_hi", C.c_float), ("hop_lo", C.c_int32),
         ("hop_hi", C.c_int32), ("hop_log_uniform", C.c_int32), ("nthreads", C.c_int32),
+        ("query_seed", C.c_uint64),
     ]
 
 

@@ -37,7 +37,7 @@ uint64_t fnv1a(uint64_t h, const void *data, size_t bytes) {
 
 // Device buffers for one host-buffer solve call.
 struct IoBuffers {
-  int32_t *src = nullptr, *dst = nullptr, *found = nullptr, *status = nullptr, *best = nullptr,
+  int32_t *src = nullptr, *dst = nullptr, *found = nullptr, *status = nullptr,
           *pareto_n = nullptr;
   float *budget = nullptr, *cost = nullptr, *delay = nullptr, *pareto_d = nullptr,
         *pareto_dl = nullptr;
@@ -48,7 +48,6 @@ struct IoBuffers {
     cudaFree(dst);
     cudaFree(found);
     cudaFree(status);
-    cudaFree(best);
     cudaFree(pareto_n);
     cudaFree(budget);
     cudaFree(cost);
@@ -106,7 +105,7 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
   int round_cap = std::min(1024, 4 * c.block_threads);
   if (c.split_threshold < 0) return fail(VINE_ERR_INVALID, "split_threshold must be >= 0");
   if (c.split_threshold > 0) round_cap = std::max(32, std::min(round_cap, c.split_threshold));
-  out->width0 = c.bucket_width > 0.0f ? c.bucket_width : std::max(1.0f, 4.0f * g->mean_len);
+  out->width0 = c.bucket_width > 0.0f ? c.bucket_width : std::max(1.0f, g->mean_len);
   out->round_cap = round_cap;
   out->slots = 0;
   if (c.engine == VINE_ENGINE_BATCH) VINE_TRY(batch_slots(g, c, round_cap, &out->slots));
@@ -148,7 +147,7 @@ int vine_graph_create(int32_t device, int32_t n, int64_t m, const int64_t *row_p
   for (int32_t u = 0; u < n; ++u)
     if (row_ptr[u + 1] < row_ptr[u]) return fail(VINE_ERR_INVALID, "row_ptr not monotone");
   bool integral = true;
-  double sum_len = 0.0;
+  double sum_len = 0.0, sum_delay = 0.0;
   for (int64_t j = 0; j < m; ++j) {
     if (col[j] < 0 || col[j] >= n) return fail(VINE_ERR_INVALID, "arc head out of range");
     if (!(len[j] >= 0.0f) || !(delay[j] >= 0.0f) || !std::isfinite(len[j]) ||
@@ -158,6 +157,7 @@ int vine_graph_create(int32_t device, int32_t n, int64_t m, const int64_t *row_p
         delay[j] >= 16777216.0f)
       integral = false;
     sum_len += len[j];
+    sum_delay += delay[j];
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -188,6 +188,7 @@ int vine_graph_create(int32_t device, int32_t n, int64_t m, const int64_t *row_p
   g->m = m;
   g->integral = integral ? 1 : 0;
   g->mean_len = m > 0 ? (float)(sum_len / (double)m) : 1.0f;
+  g->mean_delay = m > 0 ? (float)(sum_delay / (double)m) : 1.0f;
   uint64_t fp = 1469598103934665603ull;
   fp = fnv1a(fp, &n, sizeof(n));
   fp = fnv1a(fp, row32.data(), row32.size() * sizeof(int32_t));
@@ -250,10 +251,10 @@ int vine_graph_info(const vine_graph *g, int32_t *n, int64_t *m, int32_t *integr
 static int run_engine(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d_src,
                       const int32_t *d_dst, const float *d_budget, const int32_t *h_src,
                       const int32_t *h_dst, const float *h_budget, const DeviceOutputs &o,
-                      cudaStream_t s, Label **pool) {
+                      cudaStream_t s, PathOut *paths) {
   if (r.cfg.engine == VINE_ENGINE_BATCH)
-    return batch_run(g, r, nq, d_src, d_dst, d_budget, o, s, pool);
-  return plain_run(g, r, nq, h_src, h_dst, h_budget, o, s, pool);
+    return batch_run(g, r, nq, d_src, d_dst, d_budget, o, s, paths);
+  return plain_run(g, r, nq, h_src, h_dst, h_budget, o, s, paths);
 }
 
 int vine_solve_device(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst,
@@ -280,13 +281,52 @@ int vine_solve_device(vine_graph *g, int32_t nq, const int32_t *src, const int32
   o.pareto_delay = out->pareto_delay;
   o.pareto_n = out->pareto_n;
   o.pareto_stride = out->pareto_d ? out->pareto_stride : 0;
-  Label *pool = nullptr;
-  VINE_TRY(run_engine(g, r, nq, src, dst, budget, nullptr, nullptr, nullptr, o, s, &pool));
-  if (out->path_offsets && out->path) {
-    VINE_TRY(path_lengths(pool, nq, g->batch.best_idx, out->path_offsets, s));
-    // the caller guarantees path_capacity; the writer stays inside offsets
-    VINE_TRY(path_write(pool, nq, g->batch.best_idx, out->path_offsets, out->path, s));
+  VINE_TRY(batch_prepare(g, r, nq, s));
+  auto enqueue = [&]() -> int {
+    PathOut paths;
+    VINE_TRY(batch_enqueue(g, r, nq, src, dst, budget, o, s, &paths));
+    if (out->path_offsets && out->path) {
+      VINE_TRY(path_offsets(paths, nq, out->path_offsets, s));
+      // packs the paths; the caller sizes `path` (path_capacity) for the total
+      VINE_TRY(path_gather(paths, nq, out->path_offsets, out->path, s));
+    }
+    return VINE_OK;
+  };
+  if (!r.cfg.use_cuda_graph) return enqueue();
+  // Replay the captured launch sequence when the call has the same shape,
+  // buffers and configuration as the captured one; otherwise capture anew.
+  BatchWorkspace &w = g->batch;
+  uint64_t key = 1469598103934665603ull;
+  const void *ptrs[] = {src, dst, budget, out->cost, out->delay, out->found, out->status,
+                        out->stats, out->path_offsets, out->path, out->pareto_d,
+                        out->pareto_delay, out->pareto_n, stream};
+  key = fnv1a(key, &nq, sizeof(nq));
+  key = fnv1a(key, ptrs, sizeof(ptrs));
+  key = fnv1a(key, &r.cfg, sizeof(r.cfg));
+  key = fnv1a(key, &r.width0, sizeof(r.width0));
+  if (w.graph_exec == nullptr || w.graph_key != key) {
+    if (w.graph_exec) {
+      cudaGraphExecDestroy(w.graph_exec);
+      w.graph_exec = nullptr;
+    }
+    VINE_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int st = enqueue();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &graph);
+    if (st != VINE_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (e != cudaSuccess) return fail(VINE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    const cudaError_t e2 = cudaGraphInstantiate(&w.graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) {
+      w.graph_exec = nullptr;
+      return fail(VINE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2));
+    }
+    w.graph_key = key;
   }
+  VINE_CUDA_TRY(cudaGraphLaunch(w.graph_exec, s));
   return VINE_OK;
 }
 
@@ -337,7 +377,6 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
         cudaMalloc(&io.delay, sizeof(float) * k) != cudaSuccess ||
         cudaMalloc(&io.found, sizeof(int32_t) * k) != cudaSuccess ||
         cudaMalloc(&io.status, sizeof(int32_t) * k) != cudaSuccess ||
-        cudaMalloc(&io.best, sizeof(int32_t) * k) != cudaSuccess ||
         cudaMalloc(&io.offsets, sizeof(int64_t) * (k + 1)) != cudaSuccess ||
         (out->stats && cudaMalloc(&io.stats, sizeof(int64_t) * VINE_STAT_COUNT * k) != cudaSuccess) ||
         (want_pareto && (cudaMalloc(&io.pareto_d, sizeof(float) * stride * k) != cudaSuccess ||
@@ -358,14 +397,13 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
     o.pareto_delay = io.pareto_dl;
     o.pareto_n = io.pareto_n;
     o.pareto_stride = (int32_t)stride;
-    o.best_idx = io.best;
-    Label *pool = nullptr;
-    int st = run_engine(g, r, k, io.src, io.dst, io.budget, hs.data(), hd.data(), hb.data(), o, s, &pool);
+    PathOut paths;
+    int st = run_engine(g, r, k, io.src, io.dst, io.budget, hs.data(), hd.data(), hb.data(), o, s, &paths);
     if (st != VINE_OK) return bail(st);
     std::vector<int64_t> off;
     std::vector<int32_t> path;
     if (want_paths) {
-      if ((st = path_lengths(pool, k, io.best, io.offsets, s)) != VINE_OK) return bail(st);
+      if ((st = path_offsets(paths, k, io.offsets, s)) != VINE_OK) return bail(st);
       off.resize((size_t)k + 1);
       if (cudaMemcpyAsync(off.data(), io.offsets, sizeof(int64_t) * (k + 1), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
           cudaStreamSynchronize(s) != cudaSuccess)
@@ -373,7 +411,7 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
       if (off[k] > 0) {
         if (cudaMalloc(&io.path, sizeof(int32_t) * (size_t)off[k]) != cudaSuccess)
           return bail(fail(VINE_ERR_CUDA, "path allocation failed"));
-        if ((st = path_write(pool, k, io.best, io.offsets, io.path, s)) != VINE_OK) return bail(st);
+        if ((st = path_gather(paths, k, io.offsets, io.path, s)) != VINE_OK) return bail(st);
         path.resize((size_t)off[k]);
         if (cudaMemcpyAsync(path.data(), io.path, sizeof(int32_t) * (size_t)off[k], cudaMemcpyDeviceToHost, s) != cudaSuccess)
           return bail(fail(VINE_ERR_CUDA, "path download failed"));

@@ -24,7 +24,7 @@ namespace vine {
 
 constexpr int32_t kEmpty = -1;
 constexpr uint32_t kDeadBit = 0x80000000u;
-constexpr int kSpinLimit = 1 << 22;  // bounded lock spins before giving up
+constexpr int kSpinLimit = 1 << 26;  // bounded lock spins before giving up
 
 // One accepted label in the arena.  vid's top bit marks a label killed by a
 // dominating label of the same bucket.  parent is the arena index of the label
@@ -36,16 +36,79 @@ struct Label {
   int32_t parent;
 };
 
-// Per (worker, vertex) state, lazily reset through the query epoch.
-struct VState {
+// Per (worker, vertex) state, lazily reset by tags: a value is only valid
+// for the query / bucket whose tag sits beside it.  32 bytes = one sector.
+//   (epoch, sdel)  smallest delay of labels at v in finished buckets whose
+//                  table entries were folded (8-byte CAS pair)
+//   (e_del, hdel)  reverse delay distance to the sink (bounds mode, CAS pair)
+//   (bep, bmin)    bucket id and smallest delay of v's overflow chain; a
+//                  chain of an earlier bucket of the same query counts as
+//                  settled (8-byte pair, written under v's stripe lock)
+//   hlen           reverse length distance (bounds mode; valid with e_del)
+//   bhead          arena index of the newest label of v's overflow chain
+struct __align__(32) VState {
   uint32_t epoch;
-  float sdel;  // smallest delay of labels at v in finished buckets
-  float hlen;  // lower bound on the remaining cost (bounds mode)
-  float hdel;  // lower bound on the remaining delay (bounds mode)
+  float sdel;
+  uint32_t e_del;
+  float hdel;
+  uint32_t bep;
+  float bmin;
+  float hlen;
+  uint32_t bhead;
 };
 
-// Bucket-table entry.  vid == kEmpty marks a free slot; idx's top bit marks
-// a killed entry.
+// What one query sees of a vertex.
+struct VView {
+  float sdel;   // effective settled delay (+inf when none)
+  bool reach;   // bounds valid: v can lie on a feasible path
+  float hdel, hlen;
+  uint32_t bep; // chain tag
+};
+
+// qbase / bcur: first bucket id of the query and id of the open bucket.
+__device__ __forceinline__ VView view_vs(const VState *p, uint32_t epoch, uint32_t qbase,
+                                         uint32_t bcur, bool bounds) {
+  const uint4 a = __ldcg(reinterpret_cast<const uint4 *>(p));
+  const uint4 b = __ldcg(reinterpret_cast<const uint4 *>(p) + 1);
+  VView v;
+  float sd = a.x == epoch ? __uint_as_float(a.y) : INFINITY;
+  if (b.x >= qbase && b.x < bcur) sd = fminf(sd, __uint_as_float(b.y));
+  v.sdel = sd;
+  v.bep = b.x;
+  if (bounds) {
+    v.reach = a.z == epoch && __uint_as_float(b.z) < INFINITY;
+    v.hdel = __uint_as_float(a.w);
+    v.hlen = __uint_as_float(b.z);
+  } else {
+    v.reach = true;
+    v.hdel = 0.0f;
+    v.hlen = 0.0f;
+  }
+  return v;
+}
+
+// Lowers the epoch-tagged distance pair at `pair` to nd; true when improved.
+// *claimed is set when this call was the first write of the epoch.
+__device__ __forceinline__ bool relax_pair(uint32_t *pair, uint32_t epoch, float nd,
+                                           bool *claimed) {
+  unsigned long long *w = reinterpret_cast<unsigned long long *>(pair);
+  unsigned long long old = __ldcg(w);
+  for (;;) {
+    const uint32_t e = (uint32_t)old;
+    const float cur = e == epoch ? __uint_as_float((uint32_t)(old >> 32)) : INFINITY;
+    if (!(nd < cur)) return false;
+    const unsigned long long nw = ((unsigned long long)__float_as_uint(nd) << 32) | epoch;
+    const unsigned long long prev = atomicCAS(w, old, nw);
+    if (prev == old) {
+      *claimed = (e != epoch);
+      return true;
+    }
+    old = prev;
+  }
+}
+
+// Bucket-table entry (shared memory).  vid == kEmpty marks a free slot;
+// idx's top bit marks a killed entry.
 struct TEntry {
   int32_t vid;
   float d;
@@ -112,6 +175,7 @@ __device__ __forceinline__ bool with_lock(int *l, Body body) {
       atomicExch(l, 0);
       return true;
     }
+    if (it > 64) __nanosleep(32);
   }
   return false;
 }
@@ -186,28 +250,41 @@ __device__ __forceinline__ int upper_index(const int *off, int n, int e) {
 
 // ------------------------------------------------------------ bucket table
 
-// Outcome of inserting a candidate into the bucket table.
+// Outcome of inserting a candidate into the bucket store.
 enum InsertResult { kInserted = 0, kDominated = 1, kFull = 2, kLockTimeout = 3 };
 
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr uint32_t kBadIdx = 0xffffffffu;  // allocator out of arena space
+
+// Store of the labels of the open bucket.  First level: a shared-memory hash
+// table keyed by vertex (linear probing inside a short window).  When v's
+// window is full, further labels of v go to v's overflow chain in HBM: a
+// linked list through the arena (next[] parallel to it) whose head and
+// minimum delay live in v's VState, tagged with the bucket id, so chains need
+// no clearing and have no capacity limit other than the arena.
 struct BucketTable {
-  TEntry *t;         // shared-memory table
-  int log2h;         // entries = 1 << log2h
-  int probe;         // max probe window in the shared table
-  int *locks;        // striped locks (shared memory)
+  TEntry *t;           // shared-memory table
+  int log2h;           // entries = 1 << log2h
+  int probe;           // probe window in the shared table
+  int *locks;          // striped locks (shared memory)
   int lock_mask;
-  TEntry *s;         // HBM spill table of this worker
-  int log2s;
-  uint32_t *s_used;  // positions used in the spill table
-  uint32_t *s_count; // number of used spill positions (shared memory)
-  uint32_t s_limit;  // fail beyond this many spilled labels
+  VState *vs;          // per-vertex state of this worker
+  uint32_t *next;      // arena-parallel chain links
+  uint32_t epoch;      // query epoch
+  uint32_t qbase;      // first bucket id of the query
+  uint32_t bcur;       // id of the open bucket
+  unsigned long long *chain_steps;  // statistics: chain labels read
 };
 
-// Checks candidate (v, d, dl) against the labels of the open bucket at v,
-// kills the ones it dominates (marking their arena labels dead) and, when it
-// is not dominated, stores it with arena index `idx_alloc()`.  Exact: all
-// operations on one vertex are serialised by that vertex's stripe lock, and
-// a candidate is only dropped when a stored label dominates it.
-constexpr uint32_t kBadIdx = 0xffffffffu;  // allocator out of arena space
+// Dominance test of candidate (d, dl) against one stored label; kills the
+// stored label when the candidate dominates it.  Returns true when the
+// candidate is dominated.  Caller holds v's stripe lock.
+__device__ __forceinline__ bool check_one(float ed, float el, float d, float dl, bool *kill) {
+  *kill = false;
+  if (dominates(ed, el, d, dl)) return true;
+  if (dominates(d, dl, ed, el)) *kill = true;
+  return false;
+}
 
 // Body of table_insert; the caller holds v's stripe lock.
 template <typename Alloc>
@@ -228,43 +305,42 @@ __device__ InsertResult table_insert_locked(const BucketTable &bt, Label *pool, 
     if (ev != v) continue;
     const uint32_t eidx = e->idx;
     if (eidx & kDeadBit) continue;
-    const float ed = e->d, el = e->dl;
-    if (dominates(ed, el, d, dl)) return kDominated;
-    if (dominates(d, dl, ed, el)) {
+    bool kill;
+    if (check_one(e->d, e->dl, d, dl, &kill)) return kDominated;
+    if (kill) {
       e->idx = eidx | kDeadBit;
       atomicOr(reinterpret_cast<unsigned int *>(&pool[eidx].vid), kDeadBit);
     }
   }
-  const bool window_full = (free_p < 0);
-  const uint32_t smask = (1u << bt.log2s) - 1u;
-  if (window_full && *reinterpret_cast<volatile uint32_t *>(bt.s_count) > 0) {
-    // the shared window was already full when earlier labels of v arrived:
-    // they may live in the spill table
-    volatile TEntry *S = bt.s;
-    const uint32_t g0 = hash_vid(v, bt.log2s);
-    for (uint32_t q = 0; q <= smask; ++q) {
-      volatile TEntry *e = &S[(g0 + q) & smask];
-      const int32_t ev = e->vid;
-      if (ev == kEmpty) break;
-      if (ev != v) continue;
-      const uint32_t eidx = e->idx;
-      if (eidx & kDeadBit) continue;
-      const float ed = e->d, el = e->dl;
-      if (dominates(ed, el, d, dl)) return kDominated;
-      if (dominates(d, dl, ed, el)) {
-        e->idx = eidx | kDeadBit;
-        atomicOr(reinterpret_cast<unsigned int *>(&pool[eidx].vid), kDeadBit);
+  // labels of v beyond the shared window live in v's overflow chain; the
+  // window only fills up during a bucket, so a window with a free slot
+  // means v has no chain in this bucket
+  volatile VState *vs = &bt.vs[v];
+  const uint32_t bep = vs->bep;
+  const bool live_chain = (free_p < 0) && bep == bt.bcur;
+  if (live_chain) {
+    uint32_t steps = 0;
+    for (uint32_t k = vs->bhead; k != kNone; k = __ldcg(&bt.next[k])) {
+      ++steps;
+      const int4 raw = __ldcg(reinterpret_cast<const int4 *>(&pool[k]));
+      if (raw.x & (int)kDeadBit) continue;
+      bool kill;
+      if (check_one(__int_as_float(raw.y), __int_as_float(raw.z), d, dl, &kill)) {
+        if (bt.chain_steps) atomicAdd(bt.chain_steps, (unsigned long long)steps);
+        return kDominated;
       }
+      if (kill) atomicOr(reinterpret_cast<unsigned int *>(&pool[k].vid), kDeadBit);
     }
+    if (bt.chain_steps) atomicAdd(bt.chain_steps, (unsigned long long)steps);
   }
-  // not dominated: claim a slot (labels of other vertices may race for it)
-  if (!window_full) {
+  // not dominated: claim a window slot (labels of other vertices may race)
+  if (free_p >= 0) {
     for (int p = free_p; p < bt.probe; ++p) {
       TEntry *e = &bt.t[(h0 + p) & hmask];
       if (atomicCAS(&e->vid, kEmpty, v) == kEmpty) {
         const uint32_t idx = idx_alloc();
         if (idx == kBadIdx) {
-          e->idx = kDeadBit;  // keeps the probe chain intact; never expanded
+          e->idx = kDeadBit;  // keeps the probe run intact; never expanded
           return kFull;
         }
         e->d = d;
@@ -276,32 +352,26 @@ __device__ InsertResult table_insert_locked(const BucketTable &bt, Label *pool, 
       }
     }
   }
-  // spill to the HBM table of this worker
-  const uint32_t cnt = atomicAdd(bt.s_count, 1u);
-  if (cnt >= bt.s_limit) {
-    atomicSub(bt.s_count, 1u);
-    return kFull;
+  // window full: push onto v's overflow chain in HBM
+  const uint32_t idx = idx_alloc();
+  if (idx == kBadIdx) return kFull;
+  float bmin = dl;
+  uint32_t head = kNone;
+  if (bep == bt.bcur) {
+    head = vs->bhead;
+    bmin = fminf(bmin, vs->bmin);
+  } else if (bep >= bt.qbase && bep < bt.bcur) {
+    settle(const_cast<VState *>(vs), bt.epoch, vs->bmin);
   }
-  const uint32_t g0 = hash_vid(v, bt.log2s);
-  for (uint32_t q = 0; q <= smask; ++q) {
-    const uint32_t pos = (g0 + q) & smask;
-    TEntry *e = &bt.s[pos];
-    if (atomicCAS(&e->vid, kEmpty, v) == kEmpty) {
-      bt.s_used[cnt] = pos;
-      const uint32_t idx = idx_alloc();
-      if (idx == kBadIdx) {
-        e->idx = kDeadBit;
-        return kFull;
-      }
-      e->d = d;
-      e->dl = dl;
-      e->idx = idx;
-      *out_idx = idx;
-      *spilled = true;
-      return kInserted;
-    }
-  }
-  return kFull;
+  bt.next[idx] = head;
+  vs->bhead = idx;
+  __threadfence_block();
+  // publish (bep, bmin) together for lock-free readers
+  *reinterpret_cast<volatile unsigned long long *>(&vs->bep) =
+      ((unsigned long long)__float_as_uint(bmin) << 32) | bt.bcur;
+  *out_idx = idx;
+  *spilled = true;
+  return kInserted;
 }
 
 // Checks candidate (v, d, dl) against the labels of the open bucket at v,

@@ -20,7 +20,6 @@ struct BatchWorkspace {
   int slots = 0;
   int block_threads = 0;
   int table_log2 = 0;
-  int spill_log2 = 0;
   int64_t far_cap = 0;
   int64_t near_cap = 0;
   int sink_cap = 0;
@@ -28,15 +27,19 @@ struct BatchWorkspace {
   VState *vs = nullptr;
   uint32_t *nearq = nullptr;
   Label *far = nullptr;
-  TEntry *spill = nullptr;
-  TEntry *rebuild = nullptr;  // per worker: table entries kept across a rebalance
-  Label *retry = nullptr;     // per worker: 2 lists of deferred low-key candidates
-  int64_t retry_cap = 0;
-  uint32_t *spill_used = nullptr;
   uint32_t *sinklist = nullptr;
+  uint32_t *bctr = nullptr;     // per worker bucket counter
+  uint32_t *next = nullptr;     // arena-parallel chain links
+  Label *rest = nullptr;        // per worker rest pile
+  int64_t rest_cap = 0;
+  uint2 *chunks = nullptr;      // per worker arena chunk lists
+  int max_chunks = 0;
+  int32_t *path_arena = nullptr;
+  int64_t path_cap = 0;
+  int64_t *path_start = nullptr;
+  int32_t *path_len = nullptr;
   Label *pool = nullptr;
   unsigned long long *counters = nullptr;  // [0]=pool_top [1]=queue [2]=path_top [3]=trace_top
-  int32_t *best_idx = nullptr;             // per query, capacity q_cap
   int32_t *order = nullptr;
   int64_t q_cap = 0;
   float *trace = nullptr;
@@ -51,21 +54,24 @@ struct BatchWorkspace {
 // Device buffers of the plain (whole-GPU, one query at a time) engine.
 struct PlainWorkspace {
   int32_t n = 0;
-  int table_log2 = 0;
   int64_t far_cap = 0;
-  int64_t near_cap = 0;
   int64_t pool_cap = 0;
   VState *vs = nullptr;
   uint32_t *nearq = nullptr;
   Label *far[2] = {nullptr, nullptr};
-  TEntry *table = nullptr;
-  uint32_t *table_used = nullptr;
   int *locks = nullptr;
   Label *pool = nullptr;
+  uint32_t *next = nullptr;
   uint32_t *sinklist = nullptr;
-  int sink_cap = 0;
-  unsigned long long *ctl = nullptr;  // device control block (see plain.cu)
-  unsigned long long *ctl_host = nullptr;  // pinned mirror
+  int64_t q_cap = 0;
+  int32_t *path_arena = nullptr;
+  int64_t path_cap = 0;
+  int64_t *path_start = nullptr;
+  int32_t *path_len = nullptr;
+  unsigned long long *path_top = nullptr;
+  void *st = nullptr;       // device query state
+  void *st_host = nullptr;  // pinned host mirror
+  uint32_t bctr = 0;
   uint32_t epoch_next = 1;
   void release();
 };
@@ -79,6 +85,7 @@ struct vine_graph {
   int64_t m = 0;
   int32_t integral = 0;
   float mean_len = 1.0f;
+  float mean_delay = 1.0f;
   int32_t *row = nullptr, *col = nullptr, *rrow = nullptr, *rcol = nullptr;
   float2 *w = nullptr, *rw = nullptr;
   uint64_t fingerprint = 0;
@@ -122,7 +129,14 @@ struct DeviceOutputs {
   float *pareto_delay = nullptr;
   int32_t *pareto_n = nullptr;
   int32_t pareto_stride = 0;
-  int32_t *best_idx = nullptr;  // arena index of the answer label per query
+};
+
+// Where an engine left the answer paths of the last call: query q's path is
+// arena[start[q] .. start[q] + len[q]) (device pointers).
+struct PathOut {
+  const int32_t *arena = nullptr;
+  const int64_t *start = nullptr;
+  const int32_t *len = nullptr;
 };
 
 // Resolved configuration (defaults filled in).
@@ -138,17 +152,27 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out);
 // Batch engine: solves nq queries whose inputs are on the device.
 int batch_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d_src,
               const int32_t *d_dst, const float *d_budget, const DeviceOutputs &out,
-              cudaStream_t stream, Label **pool_out);
+              cudaStream_t stream, PathOut *paths);
+
+// The two halves of batch_run: workspace / epoch bookkeeping (host work,
+// never captured) and the stream work (capturable in a CUDA graph).
+int batch_prepare(vine_graph *g, const Resolved &r, int32_t nq, cudaStream_t stream);
+int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d_src,
+                  const int32_t *d_dst, const float *d_budget, const DeviceOutputs &out,
+                  cudaStream_t stream, PathOut *paths);
 
 // Plain engine: solves the queries one at a time with the whole GPU.
 int plain_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *h_src,
               const int32_t *h_dst, const float *h_budget, const DeviceOutputs &out,
-              cudaStream_t stream, Label **pool_out);
+              cudaStream_t stream, PathOut *paths);
 
-// Path extraction from an arena: lengths (pass 1) then vertices (pass 2).
-int path_lengths(const Label *pool, int32_t nq, const int32_t *d_best_idx, int64_t *d_offsets,
-                 cudaStream_t stream);
-int path_write(const Label *pool, int32_t nq, const int32_t *d_best_idx,
-               const int64_t *d_offsets, int32_t *d_path, cudaStream_t stream);
+// Orders queries by decreasing budget class (largest first).
+int order_queries(int32_t nq, const float *d_budget, int32_t *d_order, cudaStream_t stream);
+
+// Packs the paths of `p` in query order: offsets[q] = exclusive prefix sum of
+// the lengths (offsets[nq] = total), then path[offsets[q] ..] = path of q.
+int path_offsets(const PathOut &p, int32_t nq, int64_t *d_offsets, cudaStream_t stream);
+int path_gather(const PathOut &p, int32_t nq, const int64_t *d_offsets, int32_t *d_path,
+                cudaStream_t stream);
 
 }  // namespace vine

@@ -555,15 +555,17 @@ int vine_workload_generate(const vine_workload_params *p, vine_workload **out) {
         delete w;
         return vine::fail(VINE_ERR_INVALID, "unknown workload kind");
     }
+    Rng qrng(p->query_seed);
+    Rng &qr = p->query_seed ? qrng : rng;
     if (p->hop_hi > 0) {
       if (p->hop_lo < 1 || p->hop_hi < p->hop_lo) {
         delete w;
         return vine::fail(VINE_ERR_INVALID, "bad hop range");
       }
-      gen_hop_pairs(w, rng, p->n_pairs, p->hop_lo, p->hop_hi, p->hop_log_uniform != 0,
+      gen_hop_pairs(w, qr, p->n_pairs, p->hop_lo, p->hop_hi, p->hop_log_uniform != 0,
                     p->n_alpha, p->alpha, p->alpha_lo, p->alpha_hi, nt);
     } else {
-      gen_pairs(w, rng, p->n_pairs, p->n_alpha, p->alpha, p->alpha_lo, p->alpha_hi);
+      gen_pairs(w, qr, p->n_pairs, p->n_alpha, p->alpha, p->alpha_lo, p->alpha_hi);
     }
     compute_budgets(w, 0, nt);
     *out = w;
