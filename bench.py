@@ -152,7 +152,7 @@ def algorithmic_bytes(work: dict) -> float:
 
 
 def engine_config(v, policy: str, mlp, width: float):
-    base = dict(use_bounds=1, bucket_width=width)
+    base = dict(use_bounds=1, bucket_width=width, block_threads=512, table_log2=12)
     if policy == "mlp" and mlp is not None:
         return v.Config(policy="mlp", mlp=mlp, **base)
     if policy == "fixed":
@@ -249,7 +249,7 @@ def run_vine(args):
         policy = "mlp"
     elif policy in ("auto", "mlp"):
         policy = "ar"
-    width0 = float(0.25 * w.len.mean())
+    width0 = float(0.1 * w.len.mean())
     cfg = engine_config(v, policy, mlp, width0)
     tuned = ROOT / "vine_b200" / "models" / "autotune_road264k.json"
     if tuned.exists():
@@ -272,7 +272,10 @@ def run_vine(args):
            "path": torch.empty(path_cap, dtype=torch.int32, device=dev)}
     out_nopath = {k: out[k] for k in ("cost", "delay", "found", "status")}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MiB > 126 MB L2
-    stream = torch.cuda.current_stream(dev).cuda_stream
+    # a side stream: events recorded on it time the engine's launches
+    side = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(side)
+    stream = side.cuda_stream
 
     def step():
         v.solve_device(g, src, dst, bud, out, cfg_graph, stream)

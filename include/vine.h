@@ -92,7 +92,7 @@ typedef struct {
   int32_t block_threads;   /* batch engine: threads per query worker (CTA)    */
   int32_t ctas_per_sm;     /* batch engine: resident workers per SM (0=auto)  */
   int32_t table_log2;      /* shared-memory bucket table entries (log2)       */
-  int32_t spill_log2;      /* per-worker HBM spill table entries (log2)       */
+  int32_t spill_log2;      /* reserved (overflow chains have no fixed size)   */
   float bucket_width;      /* bucket width in cost units (0 = auto)           */
   int32_t split_threshold; /* max labels expanded per round (0 = auto)        */
   int64_t pool_labels;     /* label arena capacity (0 = auto)                 */
@@ -150,11 +150,13 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
                const float *budget, const vine_config *cfg, vine_results *out);
 
 /* Device-resident variant: src/dst/budget and every output pointer are device
- * pointers, work is enqueued on `stream` (cudaStream_t, may be NULL) and the
- * call returns without waiting.  out->path / path_offsets must be device
- * buffers sized by the caller (path_capacity); paths are packed in completion
- * order and path_offsets[q] holds the start, out->stats etc. as above.
- * Not retried on capacity errors. */
+ * pointers; work is enqueued on `stream` (a cudaStream_t; NULL means the
+ * legacy default stream) and the call returns without waiting.  Paths are
+ * packed in query order: out->path_offsets (nq+1 entries) receives their
+ * offsets and out->path the vertices; the caller sizes `path` (up to the
+ * number of vertices per query).  With cfg->use_cuda_graph the launch
+ * sequence is captured once and replayed while the call's shape, buffers and
+ * configuration stay the same.  Not retried on capacity errors. */
 int vine_solve_device(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst,
                       const float *budget, const vine_config *cfg, vine_results *out,
                       void *stream);

@@ -46,7 +46,7 @@ def test_config_defaults_and_names():
     c = v.Config(engine="plain", mode="pareto", policy="ar", bucket_width=50.0)
     d = v.config_dict(c)
     assert d["engine"] == 1 and d["mode"] == 1 and d["policy"] == 1
-    assert d["bucket_width"] == 50.0 and d["block_threads"] == 256
+    assert d["bucket_width"] == 50.0 and d["block_threads"] == 512
     with pytest.raises(TypeError):
         v.Config(not_a_field=1)
 

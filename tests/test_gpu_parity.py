@@ -18,6 +18,7 @@ CONFIGS = {
     "batch_wide": dict(engine="batch", bucket_width=100000.0),
     "batch_narrow": dict(engine="batch", bucket_width=1.0, block_threads=128),
     "batch_bounds": dict(engine="batch", use_bounds=1),
+    "batch_bounds_narrow": dict(engine="batch", use_bounds=1, bucket_width=5.0, block_threads=256),
     "plain": dict(engine="plain"),
     "plain_bounds": dict(engine="plain", use_bounds=1),
 }
@@ -97,3 +98,44 @@ def test_invalid_queries_get_status(graphs):
     assert res.status[0] == 0 and res.found[0] == 1 and res.cost[0] == 12
     assert res.status[1] == v._lib.VINE_ERR_INVALID and res.found[1] == 0
     assert res.status[2] == v._lib.VINE_ERR_INVALID
+
+
+@pytest.mark.parametrize("use_graph", [0, 1])
+@pytest.mark.parametrize("name", ["road_small", "road_batch_small"])
+def test_device_entry_matches_reference(graphs, name, use_graph):
+    """vine_solve_device (device buffers, caller's stream, optionally a
+    captured CUDA graph replayed on the second call) gives the same answers
+    and packed paths as the host entry and the reference."""
+    import torch
+    import vine_b200 as v
+    fx, g = graphs(name)
+    nq = len(fx["queries"])
+    dev = torch.device("cuda", 0)
+    src = torch.from_numpy(np.asarray(fx["src"], np.int32)).to(dev)
+    dst = torch.from_numpy(np.asarray(fx["dst"], np.int32)).to(dev)
+    bud = torch.from_numpy(np.asarray(fx["budget"], np.float32)).to(dev)
+    out = {"cost": torch.empty(nq, dtype=torch.float32, device=dev),
+           "delay": torch.empty(nq, dtype=torch.float32, device=dev),
+           "found": torch.empty(nq, dtype=torch.int32, device=dev),
+           "status": torch.empty(nq, dtype=torch.int32, device=dev),
+           "path_offsets": torch.empty(nq + 1, dtype=torch.int64, device=dev),
+           "path": torch.empty(nq * 4096, dtype=torch.int32, device=dev)}
+    cfg = v.Config(engine="batch", use_bounds=1, use_cuda_graph=use_graph)
+    side = torch.cuda.Stream(dev)
+    host = v.solve(g, fx["src"], fx["dst"], fx["budget"], cfg)
+    for _ in range(2):
+        for t in out.values():
+            t.fill_(-7)
+        with torch.cuda.stream(side):
+            v.solve_device(g, src, dst, bud, out, cfg, side.cuda_stream)
+        side.synchronize()
+        r = v.Results(cost=out["cost"].cpu().numpy(), delay=out["delay"].cpu().numpy(),
+                      found=out["found"].cpu().numpy(), status=out["status"].cpu().numpy())
+        r.path_offsets = out["path_offsets"].cpu().numpy()
+        r.path_vertices = out["path"].cpu().numpy()
+        for q, expect in enumerate(fx["queries"]):
+            check_result(fx, r, q, expect)
+        assert np.array_equal(r.cost, host.cost) and np.array_equal(r.found, host.found)
+        assert np.array_equal(r.path_offsets, host.path_offsets)
+        total = int(r.path_offsets[nq])
+        assert np.array_equal(r.path_vertices[:total], host.path_vertices[:total])

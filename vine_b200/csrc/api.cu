@@ -82,9 +82,9 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
     return fail(VINE_ERR_INVALID, "lower bounds prune the Pareto set; use VINE_MODE_OPTIMAL");
   if (c.use_bounds && !g->integral)
     return fail(VINE_ERR_INVALID, "lower bounds need integral weights below 2^24");
-  if (c.block_threads == 0) c.block_threads = 256;
-  if (c.block_threads < 64 || c.block_threads > 1024 || c.block_threads % 32)
-    return fail(VINE_ERR_INVALID, "block_threads must be a multiple of 32 in [64, 1024]");
+  if (c.block_threads == 0) c.block_threads = 512;
+  if (c.block_threads < 64 || c.block_threads > 512 || c.block_threads % 32)
+    return fail(VINE_ERR_INVALID, "block_threads must be a multiple of 32 in [64, 512]");
   if (c.table_log2 == 0) c.table_log2 = 11;
   if (c.table_log2 < 6 || c.table_log2 > 13) return fail(VINE_ERR_INVALID, "table_log2 in [6, 13]");
   if (c.spill_log2 == 0) c.spill_log2 = 16;
@@ -97,8 +97,10 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
   if (c.pool_labels == 0) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    int64_t want = (int64_t)(free_b / 8 / sizeof(Label));
-    c.pool_labels = std::min<int64_t>(want, int64_t(1) << 28);
+    // arena + chain links: 20 bytes per label; workers keep the chunks of
+    // their largest query, so the arena is sized for one heavy query each
+    int64_t want = (int64_t)(free_b * 2 / 5 / (sizeof(Label) + sizeof(uint32_t)));
+    c.pool_labels = std::min<int64_t>(want, (int64_t(1) << 31) - (int64_t(1) << 20));
   }
   if (c.pool_labels < 1024 || c.pool_labels > (int64_t(1) << 31) - (int64_t(1) << 20))
     return fail(VINE_ERR_INVALID, "pool_labels out of range");
@@ -129,7 +131,7 @@ void vine_config_default(vine_config *cfg) {
   cfg->mode = VINE_MODE_OPTIMAL;
   cfg->policy = VINE_POLICY_FIXED;
   cfg->use_bounds = 0;
-  cfg->block_threads = 256;
+  cfg->block_threads = 512;
   cfg->table_log2 = 11;
   cfg->spill_log2 = 16;
   cfg->use_cuda_graph = 0;
@@ -270,7 +272,7 @@ int vine_solve_device(vine_graph *g, int32_t nq, const int32_t *src, const int32
   VINE_TRY(resolve_config(g, cfg, &r));
   if (r.cfg.engine != VINE_ENGINE_BATCH)
     return fail(VINE_ERR_INVALID, "vine_solve_device runs the batch engine only");
-  cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+  cudaStream_t s = (cudaStream_t)stream;  // NULL: the legacy default stream
   DeviceOutputs o;
   o.cost = out->cost;
   o.delay = out->delay;

@@ -105,9 +105,9 @@ extern "C" int vine_autotune(vine_graph *g, int32_t nq, const int32_t *src, cons
   cudaMemcpy(d_dst, dst, 4 * (size_t)nq, cudaMemcpyHostToDevice);
   cudaMemcpy(d_budget, budget, 4 * (size_t)nq, cudaMemcpyHostToDevice);
   std::vector<Candidate> cands;
-  for (int bt : {128, 256, 512})
-    for (int tl : {10, 11, 12})
-      for (float wm : {1.0f, 2.0f, 4.0f, 8.0f}) cands.push_back({bt, tl, 0, wm});
+  for (int bt : {256, 512})
+    for (int tl : {11, 12})
+      for (float wm : {0.1f, 0.25f, 0.5f}) cands.push_back({bt, tl, 0, wm});
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);

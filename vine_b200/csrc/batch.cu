@@ -114,7 +114,7 @@ __device__ void cta_reverse_search(Ctx &c, const RoundBuf &rb, int which, float 
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(1024) batch_kernel(SearchParams P) {
+__global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int H = 1 << P.table_log2;
   const int NL = 1 << P.lock_log2;
@@ -326,7 +326,10 @@ __global__ void __launch_bounds__(1024) batch_kernel(SearchParams P) {
             __syncthreads();
             if (valid) {
               const float f = key_of(c, item.vid, item.d);
-              if (f < st.band_hi) {
+              if (P.mode == VINE_MODE_OPTIMAL &&
+                  f > key_d(*reinterpret_cast<volatile unsigned long long *>(&st.inc_key))) {
+                // beaten by the incumbent: cannot lead to a better answer
+              } else if (f < st.band_hi) {
                 push_far(c, item, f);
               } else {
                 const uint32_t w = warp_agg_inc(&st.rest_wpos);
@@ -511,7 +514,7 @@ static int ensure_batch_workspace(vine_graph *g, const Resolved &r, int32_t nq) 
     VINE_CUDA_TRY(cudaMemset(w.vs, 0, sizeof(VState) * n * r.slots));
     VINE_CUDA_TRY(cudaMalloc(&w.nearq, sizeof(uint32_t) * (size_t)near_cap * r.slots));
     VINE_CUDA_TRY(cudaMalloc(&w.far, sizeof(Label) * (size_t)c.far_capacity * r.slots));
-    w.rest_cap = c.far_capacity;
+    w.rest_cap = 4 * c.far_capacity;
     VINE_CUDA_TRY(cudaMalloc(&w.rest, sizeof(Label) * (size_t)w.rest_cap * r.slots));
     w.max_chunks = 4096;
     VINE_CUDA_TRY(cudaMalloc(&w.chunks, sizeof(uint2) * (size_t)w.max_chunks * r.slots));
@@ -629,6 +632,7 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.policy = c.policy;
   P.use_bounds = c.use_bounds;
   P.width0 = r.width0;
+  P.len_scale = std::max(1.0f, g->mean_len);
   P.delta_del = std::max(1.0f, 4.0f * g->mean_delay);
   P.delta_len = std::max(1.0f, 4.0f * g->mean_len);
   P.round_cap = r.round_cap;

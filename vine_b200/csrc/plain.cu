@@ -412,6 +412,7 @@ int plain_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *h_src
   P.policy = c.policy;
   P.use_bounds = c.use_bounds;
   P.width0 = r.width0;
+  P.len_scale = std::max(1.0f, g->mean_len);
   P.round_cap = r.round_cap;
   P.table_log2 = c.table_log2;
   P.grid_scope = 1;

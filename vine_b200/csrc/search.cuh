@@ -71,6 +71,7 @@ struct SearchParams {
   int policy;
   int use_bounds;
   float width0;
+  float len_scale;  // mean arc length: feature normalisation
   float delta_del;
   float delta_len;
   int round_cap;
@@ -290,13 +291,13 @@ __device__ __forceinline__ void push_far(Ctx &c, const Label &l, float f) {
   }
 }
 
-// Offers one label (v, nd, ndl) to the search.  from_far = true when it comes
-// from the far pile (budget already checked); returns true when a far label
-// must stay in the far pile.
-__device__ inline bool offer(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent, bool from_far) {
+// Offers one label (v, nd, ndl) to the search, given v's state view s.
+// from_far = true when it comes from the far pile (budget already checked);
+// returns true when a far label must stay in the far pile.
+__device__ inline bool offer_with(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent,
+                                  bool from_far, const VView &s) {
   const SearchParams &P = c.P;
   QueryState &st = c.st;
-  const VView s = c.view(v);
   if (!s.reach) return false;  // no feasible completion from v (bounds mode)
   const float lb_dl = ndl + s.hdel;
   if (!from_far) {
@@ -359,6 +360,14 @@ __device__ inline bool offer(Ctx &c, int32_t v, float nd, float ndl, uint32_t pa
   return false;
 }
 
+__device__ inline bool offer(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent, bool from_far) {
+  return offer_with(c, v, nd, ndl, parent, from_far, c.view(v));
+}
+
+// Items per thread whose independent global loads are issued together before
+// any of them is used (hides HBM latency on the sparse gathers of a round).
+constexpr int kBatch = 4;
+
 // Expands near-queue items [first, first + n) with the calling block
 // (n <= rb.cap): loads the labels, prefix-sums their out-degrees, then every
 // thread relaxes one arc at a time (load-balanced search over the round),
@@ -368,32 +377,50 @@ __device__ inline void expand_block(Ctx &c, const RoundBuf &rb, uint32_t first, 
   QueryState &st = c.st;
   const int tid = threadIdx.x, G = blockDim.x;
   const float hi = bucket_hi(st);
-  for (int i = tid; i < n; i += G) {
-    const uint32_t idx = c.nearq[(first + (uint32_t)i) & P.near_mask];
-    const Label lab = load_label(&P.pool[idx]);
-    const int v = lab.vid & 0x7fffffff;
-    bool live = !(lab.vid & (int)kDeadBit);
-    int beg = 0, deg = 0;
-    if (live) {
-      const VView s = P.use_bounds ? c.view(v) : VView{0.0f, true, 0.0f, 0.0f, 0u};
-      const float f = lab.d + s.hlen;
-      if (!(f < hi)) live = false;
-      if (live && P.mode == VINE_MODE_OPTIMAL) {
-        const uint64_t key = pack_key(f, lab.dl + s.hdel);
-        if (key >= *reinterpret_cast<volatile unsigned long long *>(&st.inc_key)) live = false;
+  for (int i0 = tid; i0 < n; i0 += G * kBatch) {
+    uint32_t idx[kBatch];
+    Label lab[kBatch];
+    VView s[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int i = i0 + b * G;
+      idx[b] = i < n ? c.nearq[(first + (uint32_t)i) & P.near_mask] : 0u;
+    }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (i0 + b * G < n) lab[b] = load_label(&P.pool[idx[b]]);
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      s[b] = VView{0.0f, true, 0.0f, 0.0f, 0u};
+      if (P.use_bounds && i0 + b * G < n) s[b] = c.view(lab[b].vid & 0x7fffffff);
+    }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int i = i0 + b * G;
+      if (i >= n) break;
+      const int v = lab[b].vid & 0x7fffffff;
+      bool live = !(lab[b].vid & (int)kDeadBit);
+      int beg = 0, deg = 0;
+      if (live) {
+        const float f = lab[b].d + s[b].hlen;
+        if (!(f < hi)) live = false;
+        if (live && P.mode == VINE_MODE_OPTIMAL) {
+          const uint64_t key = pack_key(f, lab[b].dl + s[b].hdel);
+          if (key >= *reinterpret_cast<volatile unsigned long long *>(&st.inc_key)) live = false;
+        }
       }
+      if (live) {
+        beg = __ldg(&P.g.row[v]);
+        deg = __ldg(&P.g.row[v + 1]) - beg;
+        if (deg > 0) warp_agg_inc(&st.r_live);
+      }
+      rb.idx[i] = idx[b];
+      rb.vid[i] = v;
+      rb.d[i] = lab[b].d;
+      rb.dl[i] = lab[b].dl;
+      rb.beg[i] = beg;
+      rb.off[i] = deg;
     }
-    if (live) {
-      beg = __ldg(&P.g.row[v]);
-      deg = __ldg(&P.g.row[v + 1]) - beg;
-      if (deg > 0) warp_agg_inc(&st.r_live);
-    }
-    rb.idx[i] = idx;
-    rb.vid[i] = v;
-    rb.d[i] = lab.d;
-    rb.dl[i] = lab.dl;
-    rb.beg[i] = beg;
-    rb.off[i] = deg;
   }
   __syncthreads();
   const int total = block_exclusive_scan(rb.off, n, rb.scan);
@@ -407,12 +434,31 @@ __device__ inline void expand_block(Ctx &c, const RoundBuf &rb, uint32_t first, 
     __syncthreads();
     if (st.abort) return;
   }
-  for (int e = tid; e < total; e += G) {
-    const int k = upper_index(rb.off, n, e);
-    const int j = rb.beg[k] + (e - rb.off[k]);
-    const int v = __ldg(&P.g.col[j]);
-    const float2 w = __ldg(&P.g.w[j]);
-    offer(c, v, rb.d[k] + w.x, rb.dl[k] + w.y, rb.idx[k], false);
+  for (int e0 = tid; e0 < total; e0 += G * kBatch) {
+    int vv[kBatch];
+    float nd[kBatch], nl[kBatch];
+    uint32_t par[kBatch];
+    VView s[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int e = e0 + b * G;
+      vv[b] = -1;
+      if (e < total) {
+        const int k = upper_index(rb.off, n, e);
+        const int j = rb.beg[k] + (e - rb.off[k]);
+        vv[b] = __ldg(&P.g.col[j]);
+        const float2 w = __ldg(&P.g.w[j]);
+        nd[b] = rb.d[k] + w.x;
+        nl[b] = rb.dl[k] + w.y;
+        par[b] = rb.idx[k];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (vv[b] >= 0) s[b] = c.view(vv[b]);
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (vv[b] >= 0) offer_with(c, vv[b], nd[b], nl[b], par[b], false, s[b]);
   }
   __syncthreads();
 }
@@ -526,18 +572,18 @@ __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
     b.rounds = (float)st.b_rounds;
     b.total_expanded = (float)st.n_expanded;
     b.buckets = (float)st.n_buckets;
-    b.width_rel = log2f(st.width / P.width0);
+    b.width_rel = log2f(st.width / P.len_scale);
     b.dominated_frac = st.b_candidates ? (float)st.b_dominated / (float)st.b_candidates : 0.0f;
     const bool have_inc = st.inc_key != ~0ull;
     b.inc_found = have_inc ? 1.0f : 0.0f;
-    b.inc_gap = have_inc ? log2f(1.0f + fmaxf(0.0f, key_d(st.inc_key) - hi) / P.width0) : -1.0f;
+    b.inc_gap = have_inc ? log2f(1.0f + fmaxf(0.0f, key_d(st.inc_key) - hi) / P.len_scale) : -1.0f;
     const float far_min = __uint_as_float(st.far_min_bits);
-    b.far_gap = st.far_n ? log2f(1.0f + fmaxf(0.0f, far_min - hi) / P.width0) : -1.0f;
+    b.far_gap = st.far_n ? log2f(1.0f + fmaxf(0.0f, far_min - hi) / P.len_scale) : -1.0f;
     b.table_fill = (float)st.b_labels / (float)(1 << P.table_log2);
     b.spilled = st.b_spilled ? 1.0f : 0.0f;
     b.mean_degree = st.b_expanded ? (float)st.b_relaxed / (float)st.b_expanded : 0.0f;
     b.ar_delta = ar_ok ? (float)(pred - xs) : 0.0f;
-    b.budget_rel = log2f(1.0f + st.budget / P.width0);
+    b.budget_rel = log2f(1.0f + st.budget / P.len_scale);
     make_features(b, st.x);
     float width = P.width0;
     const int split = P.round_cap;

@@ -1,0 +1,185 @@
+"""Learned bucket scheduler: trace collection, training and evaluation.
+
+The batch engine chooses, at every bucket boundary of every query, the width
+of the next bucket and the split threshold (labels expanded per round).  The
+reference fixes the width from an AR forecast of bucket sizes
+(algorithm/cspp.cuh:254-284); here a 16-64-64-2 FP32 MLP may choose instead,
+evaluated by one warp inside the persistent kernel.  Its outputs only change
+the order and grouping of label expansions, so answers stay exact whatever it
+predicts (a positive width and a split >= 32 are enforced by the kernel).
+
+Training data comes from the plain method itself: the engine runs a query set
+with the fixed policy at every width in WIDTH_MULTS x split in SPLITS, with
+tracing on.  Each trace row holds the 16 features the scheduler saw when a
+bucket was opened.  For every query the setting with the fewest SM cycles
+(VINE_STAT_CYCLES) is its label; every trace row of that query, from every
+setting, becomes one training example (features -> log2(best width / base
+width), log2(best split)).  Rows from all settings keep the network from
+learning "keep the current width" from the width feature.  Training runs on
+the GPU through libvine's own forward/backward and Adam kernels.
+
+Usage: ``python -m vine_b200.scheduler [--train-config 2] [--eval-config 5]``
+writes vine_b200/models/scheduler_mlp.npy and scheduler_mlp.json.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import api as v
+
+WIDTH_MULTS = (0.05, 0.1, 0.25, 0.5, 1.0)  # bucket width / mean arc length
+SPLITS = (256, 1024)
+BASE_MULT = 0.1                            # width0 the network's output is relative to
+MODEL_DIR = Path(__file__).resolve().parent / "models"
+MODEL_NPY = MODEL_DIR / "scheduler_mlp.npy"
+MODEL_JSON = MODEL_DIR / "scheduler_mlp.json"
+
+STAT_CYCLES = 7  # VINE_STAT_CYCLES
+
+
+def base_config(mean_len: float, **kw):
+    """Batch engine settings shared by every arm of the comparison."""
+    d = dict(engine="batch", use_bounds=1, block_threads=512, table_log2=12,
+             bucket_width=BASE_MULT * mean_len)
+    d.update(kw)
+    return v.Config(**d)
+
+
+def collect(graph: v.Graph, src, dst, budget, mean_len: float):
+    """Runs every (width, split) setting with the fixed policy and tracing on.
+    Returns (cycles[setting, q], traces: list of arrays, settings)."""
+    settings = [(m, s) for m in WIDTH_MULTS for s in SPLITS]
+    cycles = np.zeros((len(settings), len(src)), np.float64)
+    traces = []
+    for k, (m, s) in enumerate(settings):
+        cfg = base_config(mean_len, policy="fixed", bucket_width=m * mean_len,
+                          split_threshold=s, trace=1)
+        r = v.solve(graph, src, dst, budget, cfg, paths=False, stats=True)
+        cycles[k] = r.stats[:, STAT_CYCLES]
+        traces.append(v.fetch_trace(graph))
+    return cycles, traces, settings
+
+
+def make_dataset(cycles, traces, settings, rows_per_setting: int = 200000, seed: int = 0):
+    """Features of every trace row -> the best setting of that row's query."""
+    best = np.argmin(cycles, axis=0)
+    rng = np.random.default_rng(seed)
+    xs, ys = [], []
+    for tr in traces:
+        if tr.shape[0] == 0:
+            continue
+        if tr.shape[0] > rows_per_setting:
+            tr = tr[rng.choice(tr.shape[0], rows_per_setting, replace=False)]
+        q = tr[:, 16].astype(np.int64)
+        m = np.array([settings[b][0] for b in best[q]], np.float32)
+        s = np.array([settings[b][1] for b in best[q]], np.float32)
+        xs.append(tr[:, :16])
+        ys.append(np.stack([np.log2(m / BASE_MULT), np.log2(s)], axis=1))
+    x = np.concatenate(xs).astype(np.float32)
+    y = np.concatenate(ys).astype(np.float32)
+    ok = np.isfinite(x).all(1) & np.isfinite(y).all(1)
+    return x[ok], y[ok]
+
+
+def train(x, y, device: int = 0, epochs: int = 30, batch: int = 512, lr: float = 1e-3,
+          seed: int = 0):
+    mlp = v.MLP(device=device, seed=seed)
+    loss0, _ = mlp.loss_grad(x[:65536], y[:65536])
+    loss = mlp.train(x, y, epochs=epochs, batch=batch, lr=lr, seed=seed)
+    return mlp, float(loss0), float(loss)
+
+
+def evaluate(graph: v.Graph, src, dst, budget, mean_len: float, mlp, repeats: int = 3,
+             answers=None):
+    """Times the batch engine under the fixed, AR and MLP policies (same base
+    width); returns {policy: {ms, cycles, expanded}} and checks every arm
+    returns identical costs."""
+    import torch
+    out = {}
+    ref = answers
+    arms = {"fixed": base_config(mean_len, policy="fixed"),
+            "ar": base_config(mean_len, policy="ar")}
+    if mlp is not None:
+        arms["mlp"] = base_config(mean_len, policy="mlp", mlp=mlp)
+    for name, cfg in arms.items():
+        v.solve(graph, src, dst, budget, cfg, paths=False)  # warm-up
+        times = []
+        for _ in range(repeats):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = v.solve(graph, src, dst, budget, cfg, paths=False, stats=True)
+            times.append((time.perf_counter() - t0) * 1e3)
+        if ref is None:
+            ref = (r.cost.copy(), r.found.copy())
+        same = bool(np.array_equal(r.found, ref[1]) and
+                    np.array_equal(np.where(r.found == 1, r.cost, 0), np.where(ref[1] == 1, ref[0], 0)))
+        out[name] = {"ms": float(np.median(times)), "cycles": float(r.stats[:, STAT_CYCLES].sum()),
+                     "cycles_max": float(r.stats[:, STAT_CYCLES].max()),
+                     "expanded": int(r.stats[:, 0].sum()), "rounds": int(r.stats[:, 5].sum()),
+                     "same_answers": same}
+    return out
+
+
+def save(mlp, meta: dict):
+    MODEL_DIR.mkdir(exist_ok=True)
+    np.save(MODEL_NPY, mlp.params)
+    MODEL_JSON.write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
+
+
+def load(device: int = 0):
+    """The trained scheduler (or None) and its metadata."""
+    if not MODEL_NPY.exists():
+        return None, {}
+    meta = json.loads(MODEL_JSON.read_text()) if MODEL_JSON.exists() else {}
+    return v.MLP(device=device, params=np.load(MODEL_NPY)), meta
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--train-config", type=int, default=2)
+    ap.add_argument("--eval-config", type=int, default=5)
+    ap.add_argument("--eval-queries", type=int, default=1024)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--out", default=None, help="write the evaluation JSON here")
+    a = ap.parse_args(argv)
+
+    t0 = time.time()
+    wl = v.Workload.generate(a.train_config)
+    mean_len = float(wl.len.mean())
+    g = wl.graph()
+    cycles, traces, settings = collect(g, wl.src, wl.dst, wl.budget, mean_len)
+    x, y = make_dataset(cycles, traces, settings)
+    best = np.argmin(cycles, axis=0)
+    hist = {f"{settings[k][0]}x{settings[k][1]}": int((best == k).sum()) for k in range(len(settings))}
+    mlp, loss0, loss = train(x, y, epochs=a.epochs)
+    static_best = int(np.argmin(cycles.sum(1)))
+    g.close()
+
+    ev = v.Workload.generate(a.eval_config)
+    n = min(a.eval_queries, len(ev.src))
+    sel = np.linspace(0, len(ev.src) - 1, n).astype(np.int64)
+    ge = ev.graph()
+    res = evaluate(ge, ev.src[sel], ev.dst[sel], ev.budget[sel], float(ev.len.mean()), mlp)
+    ge.close()
+    meta = {"base_mult": BASE_MULT, "train_config": a.train_config, "rows": int(x.shape[0]),
+            "loss_initial": loss0, "loss_final": loss, "epochs": a.epochs,
+            "best_setting_histogram": hist,
+            "best_static_setting": list(settings[static_best]),
+            "oracle_best_per_query_cycles": float(cycles.min(0).sum()),
+            "best_static_cycles": float(cycles[static_best].sum()),
+            "eval_config": a.eval_config, "eval_queries": n, "eval": res,
+            "seconds": time.time() - t0}
+    save(mlp, meta)
+    text = json.dumps(meta, indent=1, sort_keys=True)
+    if a.out:
+        Path(a.out).write_text(text + "\n")
+    print(text)
+
+
+if __name__ == "__main__":
+    main()
