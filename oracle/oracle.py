@@ -80,6 +80,8 @@ def _lib_ref():
         lib.ref_graph_destroy.argtypes = [vp]
         lib.ref_solve.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp,
                                   vp, C.c_int32, vp, vp]
+        lib.ref_solve_capped.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_double, vp,
+                                         vp, vp, vp, vp]
         _ref = lib
     return _ref
 
@@ -198,6 +200,26 @@ class RefSolver:
         if record_paths:
             out["paths"] = [paths[q, : plen[q]].copy() for q in range(nq)]
         return out
+
+    def solve_capped(self, src, dst, budget, nthreads: int, cap_seconds: float):
+        """Per-query wall times with a cap: returns seconds[q] (<= ~cap),
+        finished[q], and cost / delay / found of the finished queries."""
+        src = np.ascontiguousarray(src, np.int32)
+        dst = np.ascontiguousarray(dst, np.int32)
+        budget = np.ascontiguousarray(budget, np.float32)
+        nq = src.shape[0]
+        cost = np.empty(nq, np.float32)
+        delay = np.empty(nq, np.float32)
+        found = np.zeros(nq, np.int32)
+        secs = np.zeros(nq, np.float64)
+        fin = np.zeros(nq, np.int32)
+        rc = self.lib.ref_solve_capped(self.h, nq, _p(src), _p(dst), _p(budget), nthreads,
+                                       float(cap_seconds), _p(cost), _p(delay), _p(found),
+                                       _p(secs), _p(fin))
+        if rc != 0:
+            raise RuntimeError("ref_solve_capped failed")
+        return {"seconds": secs, "finished": fin.astype(bool), "cost": cost, "delay": delay,
+                "found": found.astype(bool)}
 
     def close(self):
         if self.h:

@@ -27,6 +27,7 @@
 #include <fcntl.h>
 
 #include <atomic>
+#include <chrono>
 #include <cstdint>
 #include <limits>
 #include <thread>
@@ -49,6 +50,11 @@ thread_local int tl_best_node = -1;
 thread_local bool tl_found = false;
 thread_local long long tl_expand_calls = 0;
 thread_local long long tl_dom_calls = 0;
+// optional per-query time cap: expand_cpu checks the clock every 1024 calls
+// and unwinds out of the template (its state is all in std containers)
+thread_local bool tl_capped = false;
+thread_local std::chrono::steady_clock::time_point tl_deadline;
+struct DeadlineExceeded {};
 
 inline bool lex_less(float d0, float l0, float d1, float l1) {
   return d0 < d1 || (d0 == d1 && l0 < l1);
@@ -73,6 +79,9 @@ class OracleLabel {
     son->delay = this->delay + e.delay;
     son->node = -1;
     tl_expand_calls++;
+    if (tl_capped && (tl_expand_calls & 1023) == 0 &&
+        std::chrono::steady_clock::now() > tl_deadline)
+      throw DeadlineExceeded{};
     if (tl_record) {
       son->node = (int)tl_arena->size();
       tl_arena->push_back({next_v, this->node});
@@ -184,6 +193,55 @@ void ref_graph_destroy(void *h) {
 // to /dev/null for the duration of the call.  When record_paths is set, query
 // q's path is written to paths[q * path_stride ...] and path_len[q] is set.
 // calls (optional) receives per query {expand_cpu calls, dominate_cpu calls}.
+// Timing variant for the CPU baseline: like ref_solve without paths, but
+// each query stops after cap_seconds of wall time.  seconds[q] receives the
+// query's wall time (at most about cap_seconds) and finished[q] whether it
+// ran to completion (cost / delay / found are only meaningful then).
+int ref_solve_capped(void *h, int32_t nq, const int32_t *src, const int32_t *dst,
+                     const float *budget, int32_t nthreads, double cap_seconds, float *cost,
+                     float *delay, int32_t *found, double *seconds, int32_t *finished) {
+  auto *rg = static_cast<RefGraph *>(h);
+  if (!rg || nq < 0 || !(cap_seconds > 0.0)) return -1;
+  if (nthreads < 1) nthreads = 1;
+  fflush(stdout);
+  std::cout.flush();
+  int saved = dup(1);
+  int devnull = open("/dev/null", O_WRONLY);
+  if (saved >= 0 && devnull >= 0) dup2(devnull, 1);
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    for (;;) {
+      int q = next.fetch_add(1);
+      if (q >= nq) break;
+      const auto t0 = std::chrono::steady_clock::now();
+      tl_capped = true;
+      tl_deadline = t0 + std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+                             std::chrono::duration<double>(cap_seconds));
+      finished[q] = 1;
+      try {
+        run_one(rg->g, src[q], dst[q], budget[q], false, &cost[q], &delay[q], &found[q],
+                nullptr, 0, nullptr, nullptr);
+      } catch (const DeadlineExceeded &) {
+        finished[q] = 0;
+        found[q] = 0;
+        cost[q] = delay[q] = std::numeric_limits<float>::quiet_NaN();
+        tl_arena = nullptr;
+      }
+      tl_capped = false;
+      seconds[q] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nthreads; ++t) pool.emplace_back(worker);
+  for (auto &t : pool) t.join();
+  std::cout.flush();
+  fflush(stdout);
+  if (saved >= 0 && devnull >= 0) dup2(saved, 1);
+  if (saved >= 0) close(saved);
+  if (devnull >= 0) close(devnull);
+  return 0;
+}
+
 int ref_solve(void *h, int32_t nq, const int32_t *src, const int32_t *dst, const float *budget,
               int32_t nthreads, int32_t record_paths, float *cost, float *delay, int32_t *found,
               int32_t *paths, int32_t path_stride, int32_t *path_len, int64_t *calls) {
