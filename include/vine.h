@@ -181,6 +181,28 @@ int vine_mlp_forward(const vine_mlp *m, int32_t n, const float *x, float *y);
  * computed by the GPU forward + backward kernels (host buffers). */
 int vine_mlp_loss_grad(const vine_mlp *m, int32_t n, const float *x, const float *y_target,
                        float *loss, float *grad);
+/* No-allocation variant of vine_mlp_loss_grad (this entry point has no
+ * counterpart in the reference, which has no learned scheduler).  Same
+ * arguments and results, plus `stream` (a cudaStream_t; NULL = the legacy
+ * default stream): the inputs are staged into a fixed device scratch area
+ * that is part of the library image, the forward + backward kernel runs on
+ * `stream`, and the call waits for that stream only.  It makes no device
+ * allocation and frees nothing.  It exists for callers that must not
+ * allocate: a loop that refines the scheduler while a batch solve is running
+ * on another stream (cudaFree waits for all work on the device, which would
+ * stall it behind a persistent kernel that runs for seconds), and processes
+ * whose HBM is already handed to the label arena.
+ * Limits: 1 <= n <= VINE_MLP_NOALLOC_MAX_ROWS, else VINE_ERR_INVALID with the
+ * limit in vine_last_error().  The scratch area is one per device and per
+ * process: calls that overlap in time on the same device (other threads or
+ * streams) race on it and must be serialised by the caller.  The first call
+ * on each device looks the scratch address up (cudaGetSymbolAddress); make
+ * that first call before any stream capture begins.  The gradient and loss
+ * accumulators in the scratch area are zeroed by every call on `stream`
+ * before the kernel, so nothing has to start at zero on the caller's side. */
+#define VINE_MLP_NOALLOC_MAX_ROWS 4096
+int vine_mlp_loss_grad_noalloc(const vine_mlp *m, int32_t n, const float *x,
+                               const float *y_target, float *loss, float *grad, void *stream);
 /* `epochs` passes of mini-batch Adam over (x, y_target) on the GPU; returns
  * the final mean loss.  Mini-batches are drawn in a seeded order. */
 int vine_mlp_train(vine_mlp *m, int32_t n, const float *x, const float *y_target,

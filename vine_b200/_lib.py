@@ -92,6 +92,8 @@ SIGNATURES = {
     "vine_mlp_forward": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "vine_mlp_loss_grad": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p]),
+    "vine_mlp_loss_grad_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]),
     "vine_mlp_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                  C.c_int32, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
     "vine_trace_fetch": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_void_p, C.c_int64]),

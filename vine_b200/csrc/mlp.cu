@@ -14,7 +14,9 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <random>
+#include <string>
 #include <vector>
 
 namespace vine {
@@ -330,6 +332,83 @@ int vine_mlp_train(vine_mlp *m, int32_t n, const float *x, const float *y_target
   float l = 0.0f;
   VINE_CUDA_TRY(cudaMemcpy(&l, dL.p, sizeof(float), cudaMemcpyDeviceToHost));
   if (final_loss) *final_loss = l;
+  return VINE_OK;
+}
+
+// ------------------------------------------- no-allocation loss / gradient
+//
+// Callers that may not allocate device memory (a scheduler-refinement loop
+// running beside a seconds-long batch solve, where cudaFree would wait for
+// the whole device; a process whose HBM the label arena already holds) use
+// vine_mlp_loss_grad_noalloc.  Its staging buffers live in one fixed array
+// in the library image instead of cudaMalloc'd memory.
+//
+// Scratch layout (floats; every region starts on a 256-byte boundary):
+//   [0]                          loss accumulator      (zeroed by each call)
+//   [kNaGrad, +kMlpParams)       gradient accumulator  (zeroed by each call)
+//   [kNaX, +maxrows * 16)        x rows                (overwritten by each call)
+//   [kNaT, +maxrows * 2)         targets               (overwritten by each call)
+
+}  // extern "C"
+
+namespace vine {
+namespace {
+
+constexpr int kNaMaxRows = VINE_MLP_NOALLOC_MAX_ROWS;
+constexpr size_t kNaAlign = 64;  // floats: 256 bytes
+constexpr size_t kNaGrad = kNaAlign;
+constexpr size_t kNaX = kNaGrad + ((kMlpParams + kNaAlign - 1) / kNaAlign) * kNaAlign;
+constexpr size_t kNaT = kNaX + (size_t)kNaMaxRows * kFeat;
+constexpr size_t kNaFloats = kNaT + (size_t)kNaMaxRows * kOut;  // 79,168 floats = 309 KiB
+
+static __device__ __align__(256) float g_noalloc_scratch[kNaFloats];
+
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mu;
+float *g_na_ptr[kNaMaxDevices] = {};
+
+// Device address of the scratch array on `device` (the current device),
+// looked up once per device.
+int noalloc_scratch(int device, float **out) {
+  if (device < 0 || device >= kNaMaxDevices) return fail(VINE_ERR_INVALID, "device out of range");
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  if (g_na_ptr[device] == nullptr) {
+    float *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return fail(VINE_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") +
+                                     cudaGetErrorString(e));
+    g_na_ptr[device] = p;
+  }
+  *out = g_na_ptr[device];
+  return VINE_OK;
+}
+
+}  // namespace
+}  // namespace vine
+
+extern "C" {
+
+int vine_mlp_loss_grad_noalloc(const vine_mlp *m, int32_t n, const float *x,
+                               const float *y_target, float *loss, float *grad, void *stream) {
+  if (!m || !x || !y_target || !loss || !grad) return fail(VINE_ERR_INVALID, "bad arguments");
+  if (n < 1 || n > kNaMaxRows)
+    return fail(VINE_ERR_INVALID, "vine_mlp_loss_grad_noalloc: n = " + std::to_string(n) +
+                                      " rows, allowed 1.." + std::to_string(kNaMaxRows) +
+                                      " (VINE_MLP_NOALLOC_MAX_ROWS)");
+  VINE_CUDA_TRY(cudaSetDevice(m->device));
+  float *scratch = nullptr;
+  VINE_TRY(noalloc_scratch(m->device, &scratch));
+  cudaStream_t s = (cudaStream_t)stream;
+  float *dL = scratch, *dG = scratch + kNaGrad, *dX = scratch + kNaX, *dT = scratch + kNaT;
+  VINE_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(float) * kNaX, s));  // loss + gradient
+  VINE_CUDA_TRY(cudaMemcpyAsync(dX, x, sizeof(float) * (size_t)n * kFeat, cudaMemcpyHostToDevice, s));
+  VINE_CUDA_TRY(cudaMemcpyAsync(dT, y_target, sizeof(float) * (size_t)n * kOut,
+                                cudaMemcpyHostToDevice, s));
+  VINE_TRY(fb_launch(m, dX, dT, nullptr, n, 1.0f / n, dG, dL, nullptr, true, s));
+  VINE_CUDA_TRY(cudaMemcpyAsync(grad, dG, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, s));
+  VINE_CUDA_TRY(cudaMemcpyAsync(loss, dL, sizeof(float), cudaMemcpyDeviceToHost, s));
+  VINE_CUDA_TRY(cudaStreamSynchronize(s));
   return VINE_OK;
 }
 
