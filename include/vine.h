@@ -121,7 +121,10 @@ enum vine_stat {
   VINE_STAT_BOUND_ROUNDS, /* rounds of the reverse bound searches            */
   VINE_STAT_BOUND_CYCLES, /* device clock cycles of the reverse searches     */
   VINE_STAT_CHAIN_STEPS,  /* overflow-chain labels read by dominance tests   */
-  VINE_STAT_COUNT = 12
+  VINE_STAT_SPLIT_CYCLES, /* device clock cycles opening buckets (far piles) */
+  VINE_STAT_SPLIT_ITEMS,  /* far-pile labels scanned while opening buckets   */
+  VINE_STAT_POLICY_CYCLES,/* device clock cycles settling + scheduler steps  */
+  VINE_STAT_COUNT = 15
 };
 
 typedef struct {

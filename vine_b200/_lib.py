@@ -34,7 +34,7 @@ MODE_OPTIMAL, MODE_PARETO = 0, 1
 POLICY_FIXED, POLICY_AR, POLICY_MLP = 0, 1, 2
 STAT_NAMES = ["expanded", "relaxed", "inserted", "dominated", "buckets", "rounds", "spills",
               "cycles", "abort_site", "bound_rounds", "bound_cycles", "chain_steps"]
-STAT_COUNT = 12
+STAT_COUNT = 15
 MLP_IN, MLP_HIDDEN, MLP_OUT = 16, 64, 2
 MLP_PARAMS = 64 * 16 + 64 + 64 * 64 + 64 + 2 * 64 + 2
 TRACE_COLS = 20

@@ -196,6 +196,7 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
       st.n_buckets = st.n_rounds = st.n_spills = 0;
       st.n_chain_steps = 0;
       st.n_bound_rounds = st.bound_cycles = 0;
+      st.split_cycles = st.split_items = st.policy_cycles = 0;
       st.hist_n = 0;
       st.sink_n = 0;
       st.b_labels = st.b_expanded = st.b_rounds = st.b_dominated = 0;
@@ -269,6 +270,7 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
       const uint32_t avail = st.near_tail - st.near_head;
       if (avail == 0) {
         // ---- bucket finished: settle its table labels, pick the next bucket
+        const long long t_pol = clock64();
         atomicAdd(&st.b_dominated, c.c_dominated);
         atomicAdd(&st.b_candidates, c.c_candidates);
         atomicAdd(&st.b_spilled, c.c_spills);
@@ -311,9 +313,11 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
           }
           st.b_labels = st.b_expanded = st.b_rounds = st.b_dominated = 0;
           st.b_candidates = st.b_spilled = st.b_relaxed = 0;
+          st.policy_cycles += clock64() - t_pol;
         }
         __syncthreads();
         if (st.done) break;
+        const long long t_split = clock64();
         c.bt.bcur = st.bcur;
         if (st.rb_band) {
           // ---- rebuild the band from the rest pile (in place, tile by tile)
@@ -339,7 +343,10 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
             }
             __syncthreads();
           }
-          if (tid == 0) st.rest_n = st.rest_wpos;
+          if (tid == 0) {
+            st.split_items += rn;
+            st.rest_n = st.rest_wpos;
+          }
           __syncthreads();
         }
         if (tid == 0) {
@@ -369,7 +376,11 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
           __syncthreads();  // the tile's arena allocations end before the next reservation
         }
         __syncthreads();
-        if (tid == 0) st.far_n = st.far_wpos;
+        if (tid == 0) {
+          st.far_n = st.far_wpos;
+          st.split_items += fn;
+          st.split_cycles += clock64() - t_split;
+        }
         __syncthreads();
         continue;
       }
@@ -453,6 +464,9 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
         s[VINE_STAT_ABORT_SITE] = st.abort_site;
         s[VINE_STAT_BOUND_ROUNDS] = st.n_bound_rounds;
         s[VINE_STAT_BOUND_CYCLES] = st.bound_cycles;
+        s[VINE_STAT_SPLIT_CYCLES] = st.split_cycles;
+        s[VINE_STAT_SPLIT_ITEMS] = st.split_items;
+        s[VINE_STAT_POLICY_CYCLES] = st.policy_cycles;
         s[VINE_STAT_CHAIN_STEPS] = (long long)st.n_chain_steps;
       }
     }

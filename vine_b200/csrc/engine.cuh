@@ -165,13 +165,18 @@ __device__ __forceinline__ void atomic_min_float_nonneg(float *addr, float v) {
 // sit inside the spin loop: a lane that took the lock finishes and releases
 // it before it can reach any reconvergence point where it might wait for a
 // lane of its own warp that is still spinning on the same lock.
+// gpu_scope: the lock and the data it guards are shared by several CTAs (the
+// plain engine's global-memory locks); the fences must then order memory for
+// the whole device, not just the block.
 template <typename Body>
-__device__ __forceinline__ bool with_lock(int *l, Body body) {
+__device__ __forceinline__ bool with_lock(int *l, Body body, bool gpu_scope = false) {
   for (int it = 0; it < kSpinLimit; ++it) {
     if (atomicCAS(l, 0, 1) == 0) {
-      __threadfence_block();
+      if (gpu_scope) __threadfence();
+      else __threadfence_block();
       body();
-      __threadfence_block();
+      if (gpu_scope) __threadfence();
+      else __threadfence_block();
       atomicExch(l, 0);
       return true;
     }
@@ -379,14 +384,16 @@ __device__ InsertResult table_insert_locked(const BucketTable &bt, Label *pool, 
 // is not dominated, stores it with arena index `idx_alloc()` (which also
 // writes the arena label, so a kill can never be overwritten).  Exact: all
 // operations on one vertex are serialised by that vertex's stripe lock, and
-// a candidate is only dropped when a stored label dominates it.
+// a candidate is only dropped when a stored label dominates it.  gpu_scope:
+// the stripe locks live in global memory and are shared by all CTAs.
 template <typename Alloc>
 __device__ InsertResult table_insert(const BucketTable &bt, Label *pool, int32_t v, float d,
                                      float dl, Alloc idx_alloc, uint32_t *out_idx,
-                                     bool *spilled) {
+                                     bool *spilled, bool gpu_scope) {
   int *lk = &bt.locks[(uint32_t)v & (uint32_t)bt.lock_mask];
   InsertResult r = kLockTimeout;
-  with_lock(lk, [&]() { r = table_insert_locked(bt, pool, v, d, dl, idx_alloc, out_idx, spilled); });
+  with_lock(lk, [&]() { r = table_insert_locked(bt, pool, v, d, dl, idx_alloc, out_idx, spilled); },
+            gpu_scope);
   return r;
 }
 

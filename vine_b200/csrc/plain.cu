@@ -257,6 +257,9 @@ __global__ void plain_finish_kernel(PlainArgs A, int q) {
       s[VINE_STAT_BOUND_ROUNDS] = 0;
       s[VINE_STAT_BOUND_CYCLES] = 0;
       s[VINE_STAT_CHAIN_STEPS] = 0;
+      s[VINE_STAT_SPLIT_CYCLES] = 0;
+      s[VINE_STAT_SPLIT_ITEMS] = 0;
+      s[VINE_STAT_POLICY_CYCLES] = 0;
     }
   }
 }

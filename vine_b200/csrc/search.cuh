@@ -92,6 +92,7 @@ struct __align__(16) QueryState {
   long long n_expanded, n_relaxed, n_inserted, n_dominated, n_buckets, n_rounds, n_spills;
   unsigned long long n_chain_steps;
   long long n_bound_rounds, bound_cycles;
+  long long split_cycles, split_items, policy_cycles;
   double hist[kHist];
   int q, src, dst;
   float budget;
@@ -263,7 +264,7 @@ __device__ inline void sink_improve(Ctx &c, int32_t v, float nd, float ndl, uint
       *ik = key;
       st.inc_idx = idx;
     }
-  });
+  }, c.P.grid_scope != 0);
   if (!ok) fail_query(st, VINE_ERR_TIMEOUT, kSiteLock);
 }
 
@@ -329,7 +330,8 @@ __device__ inline bool offer_with(Ctx &c, int32_t v, float nd, float ndl, uint32
       pool[i] = Label{v, nd, ndl, (int32_t)parent};
       return i;
     };
-    const InsertResult r = table_insert(c.bt, P.pool, v, nd, ndl, alloc, &idx, &spilled);
+    const InsertResult r =
+        table_insert(c.bt, P.pool, v, nd, ndl, alloc, &idx, &spilled, P.grid_scope != 0);
     if (r == kDominated) {
       c.c_dominated++;
       return false;
