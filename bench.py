@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--nq", type=int, default=4096)
     ap.add_argument("--policy", default="auto", choices=["auto", "fixed", "ar", "mlp"])
     ap.add_argument("--no-baselines", action="store_true", help="skip CPU / plain-GPU legs")
+    ap.add_argument("--far-capacity", type=int, default=0,
+                    help="far-pile labels per worker (0 = library default); small for captures")
+    ap.add_argument("--max-workers", type=int, default=0,
+                    help="cap on batch workers (0 = one per SM); small for profiler captures")
     ap.add_argument("--pool-labels", type=int, default=0,
                     help="label arena size (0 = 2/5 of free HBM); small for profiler captures")
     return ap.parse_args()
@@ -277,6 +281,10 @@ def run_vine(args):
     cfg_graph.use_cuda_graph = 1
     if args.pool_labels:
         cfg.pool_labels = cfg_graph.pool_labels = args.pool_labels
+    if args.far_capacity:
+        cfg.far_capacity = cfg_graph.far_capacity = args.far_capacity
+    if args.max_workers:
+        cfg.max_workers = cfg_graph.max_workers = args.max_workers
 
     src = torch.from_numpy(w.src).to(dev)
     dst = torch.from_numpy(w.dst).to(dev)

@@ -101,7 +101,8 @@ typedef struct {
   int32_t order_queries;   /* batch engine: largest budget first              */
   const vine_mlp *mlp;     /* model for VINE_POLICY_MLP                       */
   int32_t trace;           /* record per-bucket scheduler traces              */
-  int32_t reserved[7];
+  int32_t max_workers;     /* batch engine: cap on resident workers (0 = all) */
+  int32_t reserved[6];
 } vine_config;
 
 void vine_config_default(vine_config *cfg);
@@ -124,7 +125,9 @@ enum vine_stat {
   VINE_STAT_SPLIT_CYCLES, /* device clock cycles opening buckets (far piles) */
   VINE_STAT_SPLIT_ITEMS,  /* far-pile labels scanned while opening buckets   */
   VINE_STAT_POLICY_CYCLES,/* device clock cycles settling + scheduler steps  */
-  VINE_STAT_COUNT = 15
+  VINE_STAT_LOAD_CYCLES,  /* device clock cycles loading round labels + scan */
+  VINE_STAT_RELAX_CYCLES, /* device clock cycles relaxing the round's arcs   */
+  VINE_STAT_COUNT = 17
 };
 
 typedef struct {

@@ -34,7 +34,7 @@ MODE_OPTIMAL, MODE_PARETO = 0, 1
 POLICY_FIXED, POLICY_AR, POLICY_MLP = 0, 1, 2
 STAT_NAMES = ["expanded", "relaxed", "inserted", "dominated", "buckets", "rounds", "spills",
               "cycles", "abort_site", "bound_rounds", "bound_cycles", "chain_steps"]
-STAT_COUNT = 15
+STAT_COUNT = 17
 MLP_IN, MLP_HIDDEN, MLP_OUT = 16, 64, 2
 MLP_PARAMS = 64 * 16 + 64 + 64 * 64 + 64 + 2 * 64 + 2
 TRACE_COLS = 20
@@ -47,7 +47,7 @@ class vine_config(C.Structure):
         ("table_log2", C.c_int32), ("spill_log2", C.c_int32), ("bucket_width", C.c_float),
         ("split_threshold", C.c_int32), ("pool_labels", C.c_int64), ("far_capacity", C.c_int64),
         ("use_cuda_graph", C.c_int32), ("order_queries", C.c_int32), ("mlp", C.c_void_p),
-        ("trace", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("trace", C.c_int32), ("max_workers", C.c_int32), ("reserved", C.c_int32 * 6),
     ]
 
 

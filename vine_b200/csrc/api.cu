@@ -91,6 +91,7 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
   if (c.spill_log2 < 8 || c.spill_log2 > 24) return fail(VINE_ERR_INVALID, "spill_log2 in [8, 24]");
   if (!(c.bucket_width >= 0.0f) || !std::isfinite(c.bucket_width))
     return fail(VINE_ERR_INVALID, "bucket_width must be finite and >= 0");
+  if (c.max_workers < 0) return fail(VINE_ERR_INVALID, "max_workers must be >= 0");
   if (c.far_capacity == 0) c.far_capacity = int64_t(1) << 20;
   if (c.far_capacity < 1024 || c.far_capacity > (int64_t(1) << 30))
     return fail(VINE_ERR_INVALID, "far_capacity out of range");

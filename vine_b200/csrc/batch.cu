@@ -119,8 +119,10 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
   const int H = 1 << P.table_log2;
   const int NL = 1 << P.lock_log2;
   const int RC = P.round_cap;
-  TEntry *table = reinterpret_cast<TEntry *>(smem);
-  int *locks = reinterpret_cast<int *>(table + H);
+  int32_t *tv = reinterpret_cast<int32_t *>(smem);
+  float2 *tw = reinterpret_cast<float2 *>(tv + H);
+  uint32_t *ti = reinterpret_cast<uint32_t *>(tw + H);
+  int *locks = reinterpret_cast<int *>(ti + H);
   uint32_t *r_idx = reinterpret_cast<uint32_t *>(locks + NL);
   int *r_vid = reinterpret_cast<int *>(r_idx + RC);
   float *r_d = reinterpret_cast<float *>(r_vid + RC);
@@ -140,7 +142,9 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
   c.far = P.far + (size_t)slot * P.far_cap;
   c.rest = P.rest + (size_t)slot * P.rest_cap;
   c.sinks = P.sinklist + (size_t)slot * P.sink_cap;
-  c.bt.t = table;
+  c.bt.tv = tv;
+  c.bt.tw = tw;
+  c.bt.ti = ti;
   c.bt.log2h = P.table_log2;
   c.bt.probe = P.probe;
   c.bt.locks = locks;
@@ -149,7 +153,7 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
   c.bt.next = P.next;
   c.bt.chain_steps = P.stats ? &st.n_chain_steps : nullptr;
 
-  for (int i = tid; i < H; i += G) table[i].vid = kEmpty;
+  for (int i = tid; i < H; i += G) tv[i] = kEmpty;
   for (int i = tid; i < NL; i += G) locks[i] = 0;
   if (tid == 0) {
     st.chunk_fill = 0;
@@ -197,6 +201,7 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
       st.n_chain_steps = 0;
       st.n_bound_rounds = st.bound_cycles = 0;
       st.split_cycles = st.split_items = st.policy_cycles = 0;
+      st.load_cycles = st.relax_cycles = 0;
       st.hist_n = 0;
       st.sink_n = 0;
       st.b_labels = st.b_expanded = st.b_rounds = st.b_dominated = 0;
@@ -252,7 +257,10 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
           st.lo = sv.hlen;
           st.hi_bits = __float_as_uint(sv.hlen + P.width0);
           st.band_hi = sv.hlen + P.width0 * (float)P.band_mult;
-          table[hash_vid(st.src, P.table_log2)] = TEntry{st.src, 0.0f, 0.0f, idx};
+          const uint32_t s0 = group_base(st.src, P.table_log2);
+          tv[s0] = st.src;
+          tw[s0] = make_float2(0.0f, 0.0f);
+          ti[s0] = idx;
           c.nearq[0] = idx;
           st.near_head = 0;
           st.near_tail = 1;
@@ -280,10 +288,10 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
         atomicAdd((unsigned long long *)&st.n_spills, (unsigned long long)c.c_spills);
         c.c_dominated = c.c_candidates = c.c_spills = c.c_near = c.c_far = 0;
         for (int i = tid; i < H; i += G) {
-          const TEntry e = table[i];
-          if (e.vid != kEmpty) {
-            if (!(e.idx & kDeadBit)) settle(&c.vs[e.vid], st.epoch, e.dl);
-            table[i].vid = kEmpty;
+          const int32_t vid = tv[i];
+          if (vid != kEmpty) {
+            if (!(ti[i] & kDeadBit)) settle(&c.vs[vid], st.epoch, tw[i].y);
+            tv[i] = kEmpty;
           }
         }
         __syncthreads();
@@ -410,7 +418,7 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
     atomicAdd((unsigned long long *)&st.n_inserted, (unsigned long long)(c.c_near + c.c_far));
     atomicAdd((unsigned long long *)&st.n_spills, (unsigned long long)c.c_spills);
     c.c_dominated = c.c_candidates = c.c_spills = c.c_near = c.c_far = 0;
-    for (int i = tid; i < H; i += G) table[i].vid = kEmpty;
+    for (int i = tid; i < H; i += G) tv[i] = kEmpty;
     if (P.mode == VINE_MODE_PARETO && !st.abort) {
       // alive sink labels are exactly the sink's Pareto set; rank-sort them
       const uint32_t k = min(st.sink_n, (uint32_t)P.sink_cap);
@@ -467,6 +475,8 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
         s[VINE_STAT_SPLIT_CYCLES] = st.split_cycles;
         s[VINE_STAT_SPLIT_ITEMS] = st.split_items;
         s[VINE_STAT_POLICY_CYCLES] = st.policy_cycles;
+        s[VINE_STAT_LOAD_CYCLES] = st.load_cycles;
+        s[VINE_STAT_RELAX_CYCLES] = st.relax_cycles;
         s[VINE_STAT_CHAIN_STEPS] = (long long)st.n_chain_steps;
       }
     }
@@ -484,7 +494,8 @@ __global__ void epoch_kernel(unsigned long long *counters, int32_t nq) {
 }
 
 size_t batch_smem_bytes(int table_log2, int lock_log2, int round_cap) {
-  size_t b = (sizeof(TEntry) << table_log2) + (sizeof(int) << lock_log2) +
+  size_t b = ((sizeof(int32_t) + sizeof(float2) + sizeof(uint32_t)) << table_log2) +
+             (sizeof(int) << lock_log2) +
              (size_t)round_cap * 24 + kScanScratch * sizeof(int);
   b = (b + 15) & ~(size_t)15;
   return b + sizeof(QueryState) + 16;
@@ -690,6 +701,7 @@ int batch_slots(const vine_graph *g, const vine_config &c, int round_cap, int *s
   if (per_sm < 1) return fail(VINE_ERR_INVALID, "batch kernel does not fit on an SM with this configuration");
   if (c.ctas_per_sm > 0) per_sm = std::min(per_sm, c.ctas_per_sm);
   *slots = per_sm * g->sm_count;
+  if (c.max_workers > 0) *slots = std::min(*slots, c.max_workers);
   return VINE_OK;
 }
 

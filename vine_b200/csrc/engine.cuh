@@ -107,14 +107,12 @@ __device__ __forceinline__ bool relax_pair(uint32_t *pair, uint32_t epoch, float
   }
 }
 
-// Bucket-table entry (shared memory).  vid == kEmpty marks a free slot;
-// idx's top bit marks a killed entry.
-struct TEntry {
-  int32_t vid;
-  float d;
-  float dl;
-  uint32_t idx;
-};
+// Bucket-table slots in shared memory, structure of arrays: tv[s] vertex id
+// (kEmpty = free), tw[s] = (d, delay), ti[s] arena index (top bit = killed).
+// Slots form aligned groups of kGroup; a vertex hashes to one group and its
+// labels only ever occupy slots of that group, so a probe is four 16-byte
+// loads of vertex ids and a compare in registers.
+constexpr int kGroup = 16;
 
 struct DevGraph {
   int32_t n;
@@ -143,6 +141,11 @@ __device__ __forceinline__ bool dominates(float ad, float al, float bd, float bl
 
 __device__ __forceinline__ uint32_t hash_vid(int32_t v, int log2n) {
   return ((uint32_t)v * 2654435769u) >> (32 - log2n);
+}
+
+// First slot of v's group in a table of 1 << log2h slots (log2h >= 6).
+__device__ __forceinline__ uint32_t group_base(int32_t v, int log2h) {
+  return hash_vid(v, log2h - 4) << 4;
 }
 
 // Warp-aggregated increment: one atomic per group of converged lanes.
@@ -262,15 +265,17 @@ constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kBadIdx = 0xffffffffu;  // allocator out of arena space
 
 // Store of the labels of the open bucket.  First level: a shared-memory hash
-// table keyed by vertex (linear probing inside a short window).  When v's
-// window is full, further labels of v go to v's overflow chain in HBM: a
+// table keyed by vertex (one aligned group of kGroup slots per vertex).  When
+// v's group is full, further labels of v go to v's overflow chain in HBM: a
 // linked list through the arena (next[] parallel to it) whose head and
 // minimum delay live in v's VState, tagged with the bucket id, so chains need
 // no clearing and have no capacity limit other than the arena.
 struct BucketTable {
-  TEntry *t;           // shared-memory table
-  int log2h;           // entries = 1 << log2h
-  int probe;           // probe window in the shared table
+  int32_t *tv;         // shared-memory slots: vertex ids
+  float2 *tw;          //   (d, delay)
+  uint32_t *ti;        //   arena index | dead bit
+  int log2h;           // slots = 1 << log2h
+  int probe;           // 0: no shared level (every label goes to a chain)
   int *locks;          // striped locks (shared memory)
   int lock_mask;
   VState *vs;          // per-vertex state of this worker
@@ -291,73 +296,81 @@ __device__ __forceinline__ bool check_one(float ed, float el, float d, float dl,
   return false;
 }
 
-// Body of table_insert; the caller holds v's stripe lock.
+// Body of table_insert; the caller holds v's stripe lock (whose acquire
+// fence orders the plain shared-memory loads below).
 template <typename Alloc>
-__device__ InsertResult table_insert_locked(const BucketTable &bt, Label *pool, int32_t v,
-                                            float d, float dl, Alloc &idx_alloc,
-                                            uint32_t *out_idx, bool *spilled) {
-  const uint32_t hmask = (1u << bt.log2h) - 1u;
-  const uint32_t h0 = hash_vid(v, bt.log2h);
-  volatile TEntry *T = bt.t;
-  int free_p = -1;
-  for (int p = 0; p < bt.probe; ++p) {
-    volatile TEntry *e = &T[(h0 + p) & hmask];
-    const int32_t ev = e->vid;
-    if (ev == kEmpty) {
-      free_p = p;
-      break;
+__device__ __forceinline__ InsertResult table_insert_locked(const BucketTable &bt, Label *pool,
+                                                            int32_t v, float d, float dl,
+                                                            Alloc &idx_alloc, uint32_t *out_idx,
+                                                            bool *spilled) {
+  uint32_t match = 0, empty = 0, base = 0;
+  if (bt.probe) {
+    base = group_base(v, bt.log2h);
+    const int4 *g4 = reinterpret_cast<const int4 *>(bt.tv + base);
+#pragma unroll
+    for (int k = 0; k < kGroup / 4; ++k) {
+      const int4 q = g4[k];
+      const int sh = 4 * k;
+      match |= (uint32_t)(q.x == v) << sh | (uint32_t)(q.y == v) << (sh + 1) |
+               (uint32_t)(q.z == v) << (sh + 2) | (uint32_t)(q.w == v) << (sh + 3);
+      empty |= (uint32_t)(q.x == kEmpty) << sh | (uint32_t)(q.y == kEmpty) << (sh + 1) |
+               (uint32_t)(q.z == kEmpty) << (sh + 2) | (uint32_t)(q.w == kEmpty) << (sh + 3);
     }
-    if (ev != v) continue;
-    const uint32_t eidx = e->idx;
-    if (eidx & kDeadBit) continue;
-    bool kill;
-    if (check_one(e->d, e->dl, d, dl, &kill)) return kDominated;
-    if (kill) {
-      e->idx = eidx | kDeadBit;
-      atomicOr(reinterpret_cast<unsigned int *>(&pool[eidx].vid), kDeadBit);
-    }
-  }
-  // labels of v beyond the shared window live in v's overflow chain; the
-  // window only fills up during a bucket, so a window with a free slot
-  // means v has no chain in this bucket
-  volatile VState *vs = &bt.vs[v];
-  const uint32_t bep = vs->bep;
-  const bool live_chain = (free_p < 0) && bep == bt.bcur;
-  if (live_chain) {
-    uint32_t steps = 0;
-    for (uint32_t k = vs->bhead; k != kNone; k = __ldcg(&bt.next[k])) {
-      ++steps;
-      const int4 raw = __ldcg(reinterpret_cast<const int4 *>(&pool[k]));
-      if (raw.x & (int)kDeadBit) continue;
+    for (uint32_t m = match; m; m &= m - 1) {
+      const uint32_t sl = base + (uint32_t)(__ffs(m) - 1);
+      const uint32_t eidx = bt.ti[sl];
+      if (eidx & kDeadBit) continue;
+      const float2 w = bt.tw[sl];
       bool kill;
-      if (check_one(__int_as_float(raw.y), __int_as_float(raw.z), d, dl, &kill)) {
-        if (bt.chain_steps) atomicAdd(bt.chain_steps, (unsigned long long)steps);
-        return kDominated;
+      if (check_one(w.x, w.y, d, dl, &kill)) return kDominated;
+      if (kill) {
+        bt.ti[sl] = eidx | kDeadBit;
+        atomicOr(reinterpret_cast<unsigned int *>(&pool[eidx].vid), kDeadBit);
       }
-      if (kill) atomicOr(reinterpret_cast<unsigned int *>(&pool[k].vid), kDeadBit);
     }
-    if (bt.chain_steps) atomicAdd(bt.chain_steps, (unsigned long long)steps);
   }
-  // not dominated: claim a window slot (labels of other vertices may race)
-  if (free_p >= 0) {
-    for (int p = free_p; p < bt.probe; ++p) {
-      TEntry *e = &bt.t[(h0 + p) & hmask];
-      if (atomicCAS(&e->vid, kEmpty, v) == kEmpty) {
-        const uint32_t idx = idx_alloc();
-        if (idx == kBadIdx) {
-          e->idx = kDeadBit;  // keeps the probe run intact; never expanded
-          return kFull;
+  // Labels of v beyond its group live in v's overflow chain.  Slots are never
+  // freed during a bucket, so a group that still had a free slot means v has
+  // no chain in this bucket.
+  const bool had_free = empty != 0;
+  volatile VState *vs = &bt.vs[v];
+  uint32_t bep = 0;
+  if (!had_free) {
+    bep = vs->bep;
+    if (bep == bt.bcur) {
+      uint32_t steps = 0;
+      for (uint32_t k = vs->bhead; k != kNone; k = __ldcg(&bt.next[k])) {
+        ++steps;
+        const int4 raw = __ldcg(reinterpret_cast<const int4 *>(&pool[k]));
+        if (raw.x & (int)kDeadBit) continue;
+        bool kill;
+        if (check_one(__int_as_float(raw.y), __int_as_float(raw.z), d, dl, &kill)) {
+          if (bt.chain_steps) atomicAdd(bt.chain_steps, (unsigned long long)steps);
+          return kDominated;
         }
-        e->d = d;
-        e->dl = dl;
-        e->idx = idx;
-        *out_idx = idx;
-        *spilled = false;
-        return kInserted;
+        if (kill) atomicOr(reinterpret_cast<unsigned int *>(&pool[k].vid), kDeadBit);
       }
+      if (bt.chain_steps) atomicAdd(bt.chain_steps, (unsigned long long)steps);
     }
   }
-  // window full: push onto v's overflow chain in HBM
+  // not dominated: claim a free slot of the group (other vertices may race)
+  for (uint32_t m = empty; m; m &= m - 1) {
+    const uint32_t sl = base + (uint32_t)(__ffs(m) - 1);
+    if (atomicCAS(&bt.tv[sl], kEmpty, v) == kEmpty) {
+      const uint32_t idx = idx_alloc();
+      if (idx == kBadIdx) {
+        bt.ti[sl] = kDeadBit;  // never expanded, never settled
+        return kFull;
+      }
+      bt.tw[sl] = make_float2(d, dl);
+      bt.ti[sl] = idx;
+      *out_idx = idx;
+      *spilled = false;
+      return kInserted;
+    }
+  }
+  // group full: push onto v's overflow chain in HBM
+  if (had_free) bep = vs->bep;  // the group filled up while we probed it
   const uint32_t idx = idx_alloc();
   if (idx == kBadIdx) return kFull;
   float bmin = dl;
@@ -387,7 +400,7 @@ __device__ InsertResult table_insert_locked(const BucketTable &bt, Label *pool, 
 // a candidate is only dropped when a stored label dominates it.  gpu_scope:
 // the stripe locks live in global memory and are shared by all CTAs.
 template <typename Alloc>
-__device__ InsertResult table_insert(const BucketTable &bt, Label *pool, int32_t v, float d,
+__device__ __forceinline__ InsertResult table_insert(const BucketTable &bt, Label *pool, int32_t v, float d,
                                      float dl, Alloc idx_alloc, uint32_t *out_idx,
                                      bool *spilled, bool gpu_scope) {
   int *lk = &bt.locks[(uint32_t)v & (uint32_t)bt.lock_mask];

@@ -43,7 +43,9 @@ __device__ void plain_ctx(Ctx &c, const PlainArgs &A) {
   c.nearq = P.nearq;
   c.far = A.far_cur;
   c.sinks = P.sinklist;
-  c.bt.t = nullptr;
+  c.bt.tv = nullptr;
+  c.bt.tw = nullptr;
+  c.bt.ti = nullptr;
   c.bt.log2h = 0;
   c.bt.probe = 0;  // no shared-memory level: every label lives in a chain
   c.bt.locks = A.locks;
@@ -260,6 +262,8 @@ __global__ void plain_finish_kernel(PlainArgs A, int q) {
       s[VINE_STAT_SPLIT_CYCLES] = 0;
       s[VINE_STAT_SPLIT_ITEMS] = 0;
       s[VINE_STAT_POLICY_CYCLES] = 0;
+      s[VINE_STAT_LOAD_CYCLES] = 0;
+      s[VINE_STAT_RELAX_CYCLES] = 0;
     }
   }
 }

@@ -92,7 +92,7 @@ struct __align__(16) QueryState {
   long long n_expanded, n_relaxed, n_inserted, n_dominated, n_buckets, n_rounds, n_spills;
   unsigned long long n_chain_steps;
   long long n_bound_rounds, bound_cycles;
-  long long split_cycles, split_items, policy_cycles;
+  long long split_cycles, split_items, policy_cycles, load_cycles, relax_cycles;
   double hist[kHist];
   int q, src, dst;
   float budget;
@@ -249,7 +249,7 @@ __device__ inline void copy_out_path(const SearchParams &P, QueryState &st, int 
 
 // Sink label that beats the incumbent (optimal mode): stored in the arena and
 // published under a small lock so that key and arena index stay paired.
-__device__ inline void sink_improve(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent,
+__device__ __forceinline__ void sink_improve(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent,
                              uint64_t key) {
   QueryState &st = c.st;
   const uint32_t idx = atomicAdd(&st.chunk_fill, 1u);
@@ -295,7 +295,7 @@ __device__ __forceinline__ void push_far(Ctx &c, const Label &l, float f) {
 // Offers one label (v, nd, ndl) to the search, given v's state view s.
 // from_far = true when it comes from the far pile (budget already checked);
 // returns true when a far label must stay in the far pile.
-__device__ inline bool offer_with(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent,
+__device__ __forceinline__ bool offer_with(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent,
                                   bool from_far, const VView &s) {
   const SearchParams &P = c.P;
   QueryState &st = c.st;
@@ -362,7 +362,7 @@ __device__ inline bool offer_with(Ctx &c, int32_t v, float nd, float ndl, uint32
   return false;
 }
 
-__device__ inline bool offer(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent, bool from_far) {
+__device__ __forceinline__ bool offer(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent, bool from_far) {
   return offer_with(c, v, nd, ndl, parent, from_far, c.view(v));
 }
 
@@ -374,11 +374,12 @@ constexpr int kBatch = 4;
 // (n <= rb.cap): loads the labels, prefix-sums their out-degrees, then every
 // thread relaxes one arc at a time (load-balanced search over the round),
 // keeping all lanes busy for degree-2 road vertices and power-law hubs alike.
-__device__ inline void expand_block(Ctx &c, const RoundBuf &rb, uint32_t first, int n) {
+__device__ __forceinline__ void expand_block(Ctx &c, const RoundBuf &rb, uint32_t first, int n) {
   const SearchParams &P = c.P;
   QueryState &st = c.st;
   const int tid = threadIdx.x, G = blockDim.x;
   const float hi = bucket_hi(st);
+  const long long t_load = clock64();
   for (int i0 = tid; i0 < n; i0 += G * kBatch) {
     uint32_t idx[kBatch];
     Label lab[kBatch];
@@ -436,6 +437,8 @@ __device__ inline void expand_block(Ctx &c, const RoundBuf &rb, uint32_t first, 
     __syncthreads();
     if (st.abort) return;
   }
+  const long long t_relax = clock64();
+  if (tid == 0 && !P.grid_scope) st.load_cycles += t_relax - t_load;
   for (int e0 = tid; e0 < total; e0 += G * kBatch) {
     int vv[kBatch];
     float nd[kBatch], nl[kBatch];
@@ -463,6 +466,7 @@ __device__ inline void expand_block(Ctx &c, const RoundBuf &rb, uint32_t first, 
       if (vv[b] >= 0) offer_with(c, vv[b], nd[b], nl[b], par[b], false, s[b]);
   }
   __syncthreads();
+  if (tid == 0 && !P.grid_scope) st.relax_cycles += clock64() - t_relax;
 }
 
 // Reverse (sink-rooted) bounded single-criterion search, one round over
