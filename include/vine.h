@@ -102,7 +102,10 @@ typedef struct {
   const vine_mlp *mlp;     /* model for VINE_POLICY_MLP                       */
   int32_t trace;           /* record per-bucket scheduler traces              */
   int32_t max_workers;     /* batch engine: cap on resident workers (0 = all) */
-  int32_t reserved[6];
+  int32_t sync_rounds;     /* batch engine: 1 = block-synchronous expansion
+                              rounds of at most split_threshold labels;
+                              0 = warps pull labels from the bucket's queue */
+  int32_t reserved[5];
 } vine_config;
 
 void vine_config_default(vine_config *cfg);

@@ -19,6 +19,8 @@ CONFIGS = {
     "batch_narrow": dict(engine="batch", bucket_width=1.0, block_threads=128),
     "batch_bounds": dict(engine="batch", use_bounds=1),
     "batch_bounds_narrow": dict(engine="batch", use_bounds=1, bucket_width=5.0, block_threads=256),
+    "batch_sync_rounds": dict(engine="batch", use_bounds=1, sync_rounds=1),
+    "batch_sync_small": dict(engine="batch", sync_rounds=1, table_log2=6, split_threshold=64),
     "plain": dict(engine="plain"),
     "plain_bounds": dict(engine="plain", use_bounds=1),
 }

@@ -114,7 +114,226 @@ __device__ void cta_reverse_search(Ctx &c, const RoundBuf &rb, int which, float 
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
+// ----------------------------------------------------------------------------
+// Asynchronous expansion of the open bucket.  Instead of block-wide rounds,
+// every warp repeatedly takes a few entries from the near ring, expands their
+// labels (one lane per label, then the warp's arcs 32 at a time with a shuffle
+// search for each arc's label), and queues the children that stay in the
+// bucket.  Chains of labels inside a bucket (long with exact A* keys, whose
+// reduced arc costs are near zero along good paths) then advance at the
+// latency of one expansion instead of one block-wide round.
+//
+// Ring protocol: producers reserve entries with atomicAdd(near_tail), write
+// them, and publish them in reservation order by advancing near_commit;
+// consumers take entries below near_commit with a CAS on near_head.
+// `pending` counts queued labels whose expansion is not finished: children
+// are counted before their parent is uncounted, so pending == 0 with nothing
+// left to take means the bucket is finished.  Every wait is bounded.
+constexpr long long kAsyncPolls = 1ll << 26;
+constexpr uint32_t kSlab = 1024;  // arena slots a warp takes at a time
+
+__device__ __forceinline__ void async_push(Ctx &c, bool is_near, uint32_t idx, int32_t v) {
+  const SearchParams &P = c.P;
+  QueryState &st = c.st;
+  const int lane = threadIdx.x & 31;
+  const unsigned nm = __ballot_sync(0xffffffffu, is_near);
+  if (nm == 0) return;
+  const uint32_t k = (uint32_t)__popc(nm);
+  uint32_t base = 0;
+  if (lane == 0) {
+    base = atomicAdd(&st.near_tail, k);
+    atomicAdd(&st.pending, k);
+    if (base + k - *reinterpret_cast<volatile uint32_t *>(&st.near_head) > P.near_mask + 1u)
+      fail_query(st, VINE_ERR_CAPACITY, kSiteNear);  // entries still written: in bounds
+  }
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (is_near) {
+    const uint32_t rank = (uint32_t)__popc(nm & ((1u << lane) - 1u));
+    c.near_ring()[(base + rank) & P.near_mask] = make_uint2(idx, (uint32_t)v);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    __threadfence_block();
+    volatile uint32_t *cm = &st.near_commit;
+    long long polls = 0;
+    while (*cm != base) {
+      if (++polls > kAsyncPolls) {
+        fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
+        break;
+      }
+    }
+    *cm = base + k;
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void bucket_async(Ctx &c) {
+  const SearchParams &P = c.P;
+  QueryState &st = c.st;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const float hi = bucket_hi(st);
+  const uint2 *ring = c.near_ring();
+  // polls without any change of (near_commit, pending): only a stuck bucket
+  // reaches the limit, however long the other warps' expansions take
+  long long idle = 0;
+  uint32_t seen_commit = 0xffffffffu, seen_pending = 0xffffffffu;
+  for (;;) {
+    // ---- take up to 32 entries (fewer when the ring is short, so that the
+    // ---- idle warps share the work)
+    uint32_t h = 0, take = 0;
+    int stop = 0;
+    if (lane == 0) {
+      for (;;) {
+        if (*reinterpret_cast<volatile int *>(&st.abort)) {
+          stop = 1;
+          break;
+        }
+        const uint32_t cm = *reinterpret_cast<volatile uint32_t *>(&st.near_commit);
+        h = *reinterpret_cast<volatile uint32_t *>(&st.near_head);
+        if (h != cm) {
+          const uint32_t avail = cm - h;
+          take = min(32u, max(1u, (avail + (uint32_t)nw - 1u) / (uint32_t)nw));
+          if (atomicCAS(&st.near_head, h, h + take) == h) break;
+          continue;
+        }
+        const uint32_t pend = *reinterpret_cast<volatile uint32_t *>(&st.pending);
+        if (pend == 0) {
+          stop = 1;
+          break;
+        }
+        if (cm != seen_commit || pend != seen_pending) {
+          seen_commit = cm;
+          seen_pending = pend;
+          idle = 0;
+        }
+        if (++idle > kAsyncPolls) {
+          fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
+          stop = 1;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    if (__shfl_sync(FULL, stop, 0)) break;
+    h = __shfl_sync(FULL, h, 0);
+    take = __shfl_sync(FULL, take, 0);
+    __threadfence_block();  // entries below near_commit are visible
+
+    // ---- the taken labels, one per lane
+    uint32_t idx = 0;
+    float d = 0.0f, dl = 0.0f;
+    int beg = 0, deg = 0;
+    if ((uint32_t)lane < take) {
+      const uint2 e = __ldcg(&ring[(h + (uint32_t)lane) & P.near_mask]);
+      idx = e.x;
+      const int v = (int)e.y;
+      const Label lab = load_label(&P.pool[idx]);  // issued together with the loads below
+      const VView s = P.use_bounds ? c.view(v) : VView{0.0f, true, 0.0f, 0.0f, 0u};
+      const int r0 = __ldg(&P.g.row[v]);
+      const int r1 = __ldg(&P.g.row[v + 1]);
+      d = lab.d;
+      dl = lab.dl;
+      bool live = !(lab.vid & (int)kDeadBit);
+      if (live) {
+        const float f = d + s.hlen;
+        if (!(f < hi)) live = false;
+        if (live && P.mode == VINE_MODE_OPTIMAL) {
+          const uint64_t key = pack_key(f, dl + s.hdel);
+          if (key >= *reinterpret_cast<volatile unsigned long long *>(&st.inc_key)) live = false;
+        }
+      }
+      if (live) {
+        beg = r0;
+        deg = r1 - r0;
+      }
+    }
+    int incl = deg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    const int excl = incl - deg;
+    const unsigned expanded = __ballot_sync(FULL, deg > 0);
+    if (lane == 0) {
+      const uint32_t ne = (uint32_t)__popc(expanded);
+      atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_expanded), (unsigned long long)ne);
+      atomicAdd(&st.b_expanded, ne);
+      atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_relaxed), (unsigned long long)total);
+      atomicAdd(&st.b_relaxed, (uint32_t)total);
+      atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_rounds), 1ull);
+      atomicAdd(&st.b_rounds, 1u);
+    }
+
+    // ---- the arcs, 32 at a time
+    if (total > 0) {
+      bool failed = false;
+      for (int e0 = 0; e0 < total; e0 += 32) {
+        // every arc allocates at most one arena slot: keep 32 free in the slab
+        int bad = 0;
+        if (lane == 0 && st.slab_end[warp] - st.slab_fill[warp] < 32u) {
+          const uint32_t b = arena_take(P, st, kSlab);
+          if (b == kBadIdx) {
+            bad = 1;
+          } else {
+            st.slab_fill[warp] = b;
+            st.slab_end[warp] = b + kSlab;
+          }
+        }
+        if (__shfl_sync(FULL, bad, 0)) {
+          failed = true;
+          break;
+        }
+        __syncwarp();
+        c.slab_fill = &st.slab_fill[warp];
+        const int e = e0 + lane;
+        // owner label of arc e: the last lane k with excl_k <= e
+        int k = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+          const int ex = __shfl_sync(FULL, excl, (k + step) & 31);
+          if (k + step < 32 && ex <= e) k += step;
+        }
+        const int obeg = __shfl_sync(FULL, beg, k);
+        const int oex = __shfl_sync(FULL, excl, k);
+        const float od = __shfl_sync(FULL, d, k);
+        const float odl = __shfl_sync(FULL, dl, k);
+        const uint32_t oidx = __shfl_sync(FULL, idx, k);
+        uint32_t nidx = kNone;
+        int u = 0;
+        if (e < total) {
+          const int j = obeg + (e - oex);
+          u = __ldg(&P.g.col[j]);
+          const float2 w = __ldg(&P.g.w[j]);
+          const VView s = c.view(u);
+          offer_with(c, u, od + w.x, odl + w.y, oidx, false, s, &nidx);
+        }
+        async_push(c, nidx != kNone, nidx, u);
+      }
+      c.slab_fill = nullptr;
+      if (failed) break;  // query failed (abort set)
+    }
+    __syncwarp();
+    if (lane == 0) atomicSub(&st.pending, take);
+  }
+  // fold the per-thread counters into the bucket statistics
+  atomicAdd(&st.b_dominated, c.c_dominated);
+  atomicAdd(&st.b_candidates, c.c_candidates);
+  atomicAdd(&st.b_spilled, c.c_spills);
+  atomicAdd(&st.b_labels, c.c_near);
+  atomicAdd((unsigned long long *)&st.n_dominated, (unsigned long long)c.c_dominated);
+  atomicAdd((unsigned long long *)&st.n_inserted, (unsigned long long)(c.c_near + c.c_far));
+  atomicAdd((unsigned long long *)&st.n_spills, (unsigned long long)c.c_spills);
+  c.c_dominated = c.c_candidates = c.c_spills = c.c_near = c.c_far = 0;
+}
+
+// Far-pile items per thread whose loads are issued together when a bucket
+// opens (more would spill registers around the inlined insert path).
+constexpr int kSplitBatch = 2;
+
+__global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int H = 1 << P.table_log2;
   const int NL = 1 << P.lock_log2;
@@ -138,7 +357,7 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
   Ctx c(P, st);
   const RoundBuf rb{r_idx, r_vid, r_d, r_dl, r_beg, r_off, scan, RC};
   c.vs = P.vs + (size_t)slot * P.g.n;
-  c.nearq = P.nearq + (size_t)slot * (P.near_mask + 1u);
+  c.nearq = P.nearq + (size_t)slot * 2 * (P.near_mask + 1u);  // uint2 entries
   c.far = P.far + (size_t)slot * P.far_cap;
   c.rest = P.rest + (size_t)slot * P.rest_cap;
   c.sinks = P.sinklist + (size_t)slot * P.sink_cap;
@@ -158,6 +377,7 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
   if (tid == 0) {
     st.chunk_fill = 0;
     st.chunk_end = 0;
+    st.chunk_lock = 0;
     st.n_chunks = 0;
     st.cur_chunk = 0;
     st.bcur = P.bctr[slot];
@@ -185,6 +405,10 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
       st.inc_key = ~0ull;
       st.inc_idx = 0xffffffffu;
       st.inc_lock = 0;
+      st.chunk_lock = 0;
+      for (int i = 0; i < 32; ++i) st.slab_fill[i] = st.slab_end[i] = 0;
+      st.pending = 0;
+      st.near_commit = 0;
       st.far_n = 0;
       st.far_wpos = 0;
       st.far_min_bits = kInfBits;
@@ -261,7 +485,7 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
           tv[s0] = st.src;
           tw[s0] = make_float2(0.0f, 0.0f);
           ti[s0] = idx;
-          c.nearq[0] = idx;
+          c.near_ring()[0] = make_uint2(idx, (uint32_t)st.src);
           st.near_head = 0;
           st.near_tail = 1;
           st.b_labels = 1;
@@ -330,23 +554,31 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
         if (st.rb_band) {
           // ---- rebuild the band from the rest pile (in place, tile by tile)
           const uint32_t rn = st.rest_n;
-          for (uint32_t base = 0; base < rn; base += (uint32_t)G) {
-            const uint32_t i = base + tid;
-            Label item;
-            const bool valid = i < rn;
-            if (valid) item = c.rest[i];
-            __syncthreads();
-            if (valid) {
-              const float f = key_of(c, item.vid, item.d);
+          const uint32_t rtile = (uint32_t)G * kSplitBatch;
+          for (uint32_t base = 0; base < rn; base += rtile) {
+            Label item[kSplitBatch];
+            float f[kSplitBatch];
+#pragma unroll
+            for (int b = 0; b < kSplitBatch; ++b) {
+              const uint32_t i = base + (uint32_t)(b * G + tid);
+              if (i < rn) item[b] = c.rest[i];
+            }
+#pragma unroll
+            for (int b = 0; b < kSplitBatch; ++b)
+              if (base + (uint32_t)(b * G + tid) < rn) f[b] = key_of(c, item[b].vid, item[b].d);
+            __syncthreads();  // the whole tile is read before it is overwritten
+#pragma unroll
+            for (int b = 0; b < kSplitBatch; ++b) {
+              if (base + (uint32_t)(b * G + tid) >= rn) break;
               if (P.mode == VINE_MODE_OPTIMAL &&
-                  f > key_d(*reinterpret_cast<volatile unsigned long long *>(&st.inc_key))) {
+                  f[b] > key_d(*reinterpret_cast<volatile unsigned long long *>(&st.inc_key))) {
                 // beaten by the incumbent: cannot lead to a better answer
-              } else if (f < st.band_hi) {
-                push_far(c, item, f);
+              } else if (f[b] < st.band_hi) {
+                push_far(c, item[b], f[b]);
               } else {
                 const uint32_t w = warp_agg_inc(&st.rest_wpos);
-                c.rest[w] = item;
-                atomicMin(&st.rest_min_bits, __float_as_uint(f));
+                c.rest[w] = item[b];
+                atomicMin(&st.rest_min_bits, __float_as_uint(f[b]));
               }
             }
             __syncthreads();
@@ -364,21 +596,30 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
         __syncthreads();
         // ---- split the band: labels below hi enter the bucket
         const uint32_t fn = st.far_n;
-        for (uint32_t base = 0; base < fn; base += (uint32_t)G) {
-          if (tid == 0) pool_reserve(P, st, (uint32_t)G);
+        const uint32_t tile = (uint32_t)G * kSplitBatch;
+        for (uint32_t base = 0; base < fn; base += tile) {
+          if (tid == 0) pool_reserve(P, st, tile);
           __syncthreads();
           if (st.abort) break;
-          const uint32_t i = base + tid;
-          Label item;
-          const bool valid = i < fn;
-          if (valid) item = c.far[i];
+          Label item[kSplitBatch];
+          VView sv[kSplitBatch];
+#pragma unroll
+          for (int b = 0; b < kSplitBatch; ++b) {
+            const uint32_t i = base + (uint32_t)(b * G + tid);
+            if (i < fn) item[b] = c.far[i];
+          }
+#pragma unroll
+          for (int b = 0; b < kSplitBatch; ++b)
+            if (base + (uint32_t)(b * G + tid) < fn) sv[b] = c.view(item[b].vid);
           __syncthreads();  // the whole tile is read before it is overwritten
-          if (valid) {
-            const bool keep = offer(c, item.vid, item.d, item.dl, (uint32_t)item.parent, true);
-            if (keep) {
+#pragma unroll
+          for (int b = 0; b < kSplitBatch; ++b) {
+            if (base + (uint32_t)(b * G + tid) >= fn) break;
+            const Label &it = item[b];
+            if (offer_with(c, it.vid, it.d, it.dl, (uint32_t)it.parent, true, sv[b])) {
               const uint32_t w = warp_agg_inc(&st.far_wpos);
-              c.far[w] = item;
-              atomicMin(&st.far_min_bits, __float_as_uint(key_of(c, item.vid, item.d)));
+              c.far[w] = it;
+              atomicMin(&st.far_min_bits, __float_as_uint(P.use_bounds ? it.d + sv[b].hlen : it.d));
             }
           }
           __syncthreads();  // the tile's arena allocations end before the next reservation
@@ -393,6 +634,19 @@ __global__ void __launch_bounds__(512) batch_kernel(SearchParams P) {
         continue;
       }
 
+      if (!P.sync_rounds) {
+        // ---- the whole bucket, warps pulling work from the near ring
+        if (tid == 0) {
+          st.near_commit = st.near_tail;
+          st.pending = st.near_tail - st.near_head;
+        }
+        __syncthreads();
+        const long long t_async = clock64();
+        bucket_async(c);
+        __syncthreads();
+        if (tid == 0) st.relax_cycles += clock64() - t_async;
+        continue;
+      }
       // ---- one expansion round over up to split_cap near labels
       const int n_round = (int)min((uint32_t)min(RC, st.split_cap), avail);
       const uint32_t first = st.near_head;
@@ -537,7 +791,7 @@ static int ensure_batch_workspace(vine_graph *g, const Resolved &r, int32_t nq) 
     const size_t n = (size_t)g->n;
     VINE_CUDA_TRY(cudaMalloc(&w.vs, sizeof(VState) * n * r.slots));
     VINE_CUDA_TRY(cudaMemset(w.vs, 0, sizeof(VState) * n * r.slots));
-    VINE_CUDA_TRY(cudaMalloc(&w.nearq, sizeof(uint32_t) * (size_t)near_cap * r.slots));
+    VINE_CUDA_TRY(cudaMalloc(&w.nearq, sizeof(uint2) * (size_t)near_cap * r.slots));
     VINE_CUDA_TRY(cudaMalloc(&w.far, sizeof(Label) * (size_t)c.far_capacity * r.slots));
     w.rest_cap = 4 * c.far_capacity;
     VINE_CUDA_TRY(cudaMalloc(&w.rest, sizeof(Label) * (size_t)w.rest_cap * r.slots));
@@ -658,6 +912,7 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.use_bounds = c.use_bounds;
   P.width0 = r.width0;
   P.len_scale = std::max(1.0f, g->mean_len);
+  P.sync_rounds = c.sync_rounds;
   P.delta_del = std::max(1.0f, 4.0f * g->mean_delay);
   P.delta_len = std::max(1.0f, 4.0f * g->mean_len);
   P.round_cap = r.round_cap;

@@ -158,6 +158,15 @@ __device__ __forceinline__ uint32_t warp_agg_inc(uint32_t *ctr) {
   return base + (uint32_t)grp.thread_rank();
 }
 
+// Thread -> work-item order that deals consecutive items to different warps
+// (item j goes to lane j / nwarps of warp j % nwarps): a round with fewer
+// items than threads then keeps every warp busy with a few lanes instead of
+// packing the items into a few warps whose divergent lanes run one path at a
+// time.  A permutation of [0, G) for G a multiple of 32.
+__device__ __forceinline__ int spread_index(int tid, int G) {
+  return (tid & 31) * (G >> 5) + (tid >> 5);
+}
+
 __device__ __forceinline__ void atomic_min_float_nonneg(float *addr, float v) {
   // non-negative floats order like their bit patterns
   atomicMin(reinterpret_cast<unsigned int *>(addr), __float_as_uint(v));

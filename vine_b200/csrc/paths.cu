@@ -12,32 +12,56 @@ namespace vine {
 
 namespace {
 
-// Orders queries by decreasing budget class (floor(log2(budget + 1))), a
-// cheap proxy for query difficulty: the longest queries start first.
+// Orders queries by decreasing budget (classes 1/128 of an octave wide), a
+// cheap proxy for query difficulty: the longest queries start first, so the
+// persistent workers finish together (longest-processing-time-first).
+constexpr int kOrderBins = 4096;
+
+__device__ __forceinline__ int budget_bin(float b) {
+  if (!(b > 0.0f) || !isfinite(b)) return 0;
+  return min(kOrderBins - 1, (int)(log2f(b + 1.0f) * 128.0f));
+}
+
 __global__ void order_kernel(int32_t nq, const float *budget, int32_t *order) {
-  __shared__ int hist[64];
-  __shared__ int base[64];
-  for (int i = threadIdx.x; i < 64; i += blockDim.x) hist[i] = 0;
+  __shared__ int hist[kOrderBins];
+  __shared__ int warp_tot[32];
+  for (int i = threadIdx.x; i < kOrderBins; i += blockDim.x) hist[i] = 0;
   __syncthreads();
-  for (int i = threadIdx.x; i < nq; i += blockDim.x) {
-    const float b = budget[i];
-    int cls = (b > 0.0f && isfinite(b)) ? min(63, (int)log2f(b + 1.0f)) : 0;
-    atomicAdd(&hist[63 - cls], 1);
+  for (int i = threadIdx.x; i < nq; i += blockDim.x)
+    atomicAdd(&hist[kOrderBins - 1 - budget_bin(budget[i])], 1);
+  __syncthreads();
+  // exclusive scan of the histogram: each thread owns a contiguous run of bins
+  const int per = kOrderBins / blockDim.x;  // blockDim.x divides kOrderBins
+  const int b0 = threadIdx.x * per;
+  int run = 0;
+  for (int k = 0; k < per; ++k) run += hist[b0 + k];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = run;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
   }
+  if (lane == 31) warp_tot[warp] = incl;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int run = 0;
-    for (int i = 0; i < 64; ++i) {
-      base[i] = run;
-      run += hist[i];
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    int v = lane < nw ? warp_tot[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
     }
+    if (lane < nw) warp_tot[lane] = v;  // inclusive warp totals
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < nq; i += blockDim.x) {
-    const float b = budget[i];
-    int cls = (b > 0.0f && isfinite(b)) ? min(63, (int)log2f(b + 1.0f)) : 0;
-    order[atomicAdd(&base[63 - cls], 1)] = i;
+  int base = (incl - run) + (warp > 0 ? warp_tot[warp - 1] : 0);
+  for (int k = 0; k < per; ++k) {
+    const int h = hist[b0 + k];
+    hist[b0 + k] = base;
+    base += h;
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nq; i += blockDim.x)
+    order[atomicAdd(&hist[kOrderBins - 1 - budget_bin(budget[i])], 1)] = i;
 }
 
 __global__ void path_len_kernel(const int32_t *len, int32_t nq, int64_t *off) {

@@ -198,7 +198,7 @@ __global__ void plain_setup_kernel(PlainArgs A, int q, int phase) {
     vs->bhead = idx;
     *reinterpret_cast<volatile unsigned long long *>(&vs->bep) =
         ((unsigned long long)__float_as_uint(0.0f) << 32) | st.bcur;
-    c.nearq[st.near_tail & P.near_mask] = idx;
+    c.near_ring()[st.near_tail & P.near_mask] = make_uint2(idx, (uint32_t)st.src);
     st.near_tail += 1;
     st.b_labels = 1;
   }
@@ -338,7 +338,7 @@ static int ensure_plain_workspace(vine_graph *g, const Resolved &r, int32_t nq) 
     w.release();
     VINE_CUDA_TRY(cudaMalloc(&w.vs, sizeof(VState) * (size_t)g->n));
     VINE_CUDA_TRY(cudaMemset(w.vs, 0, sizeof(VState) * (size_t)g->n));
-    VINE_CUDA_TRY(cudaMalloc(&w.nearq, sizeof(uint32_t) * (size_t)kPlainNear));
+    VINE_CUDA_TRY(cudaMalloc(&w.nearq, sizeof(uint2) * (size_t)kPlainNear));
     VINE_CUDA_TRY(cudaMalloc(&w.far[0], sizeof(Label) * (size_t)far_cap));
     VINE_CUDA_TRY(cudaMalloc(&w.far[1], sizeof(Label) * (size_t)far_cap));
     VINE_CUDA_TRY(cudaMalloc(&w.locks, sizeof(int) << kPlainLockLog2));

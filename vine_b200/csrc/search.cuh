@@ -79,6 +79,7 @@ struct SearchParams {
   int lock_log2;
   int probe;
   int grid_scope;  // 1: one query spread over the whole grid (plain engine)
+  int sync_rounds; // batch engine: 1 = block-synchronous rounds, 0 = warps pull work
   const float *mlp;
   float *trace;
   unsigned long long *trace_top;
@@ -93,6 +94,9 @@ struct __align__(16) QueryState {
   unsigned long long n_chain_steps;
   long long n_bound_rounds, bound_cycles;
   long long split_cycles, split_items, policy_cycles, load_cycles, relax_cycles;
+  // arena chunk cursor: fill (low word) and end (high word) of the current
+  // chunk, also updated as one 64-bit word when warps reserve concurrently
+  uint32_t chunk_fill, chunk_end;
   double hist[kHist];
   int q, src, dst;
   float budget;
@@ -109,7 +113,11 @@ struct __align__(16) QueryState {
   int abort_site;
   int rb_band;
   uint32_t near_head, near_tail;
-  uint32_t chunk_fill, chunk_end;
+  uint32_t near_commit;  // ring entries below this are published (async mode)
+  uint32_t pending;      // labels of the open bucket not yet fully expanded
+  int chunk_lock;
+  uint32_t slab_fill[32], slab_end[32];  // per-warp arena slabs (async mode)
+
   int abort;
   int done;
   int split_cap;
@@ -160,10 +168,18 @@ struct Ctx {
   Label *rest;
   uint32_t *sinks;
   uint32_t c_dominated = 0, c_near = 0, c_far = 0, c_spills = 0, c_candidates = 0;
+  // async mode: arena slots come from this warp's slab (slab_fill points at
+  // its fill counter; the slab always has room for the 32 arcs in flight)
+  uint32_t *slab_fill = nullptr;
   __device__ Ctx(const SearchParams &p, QueryState &s) : P(p), st(s) {}
+  // One arena slot (kBadIdx when the arena is exhausted).
+  __device__ __forceinline__ uint32_t alloc_one();
   __device__ VView view(int v) const {
     return view_vs(&vs[v], st.epoch, st.qbase, st.bcur, P.use_bounds != 0);
   }
+  // Forward-search ring entries: (arena index, vertex).  The reverse bound
+  // searches use the same memory as a ring of vertex ids.
+  __device__ __forceinline__ uint2 *near_ring() const { return reinterpret_cast<uint2 *>(nearq); }
 };
 
 __device__ __forceinline__ float key_of(const Ctx &c, int32_t vid, float d) {
@@ -178,8 +194,40 @@ __device__ __forceinline__ void fail_query(QueryState &st, int status, int site)
 enum AbortSite {
   kSiteArena = 1, kSiteArenaAlloc = 2, kSiteNear = 3, kSiteBand = 4, kSiteRest = 5,
   kSiteSink = 6, kSiteLock = 7, kSiteRounds = 8, kSitePath = 9, kSiteChunks = 10,
-  kSiteInvalid = 11
+  kSiteInvalid = 11, kSiteAsync = 12
 };
+
+// Next arena chunk with room for `need` labels: a kept chunk of the worker
+// (reused across its queries) or a new one from the global arena.  Caller has
+// exclusive use of the chunk list (one thread between barriers, or the
+// chunk lock).  Returns false (query failed) when the arena is exhausted.
+__device__ inline bool next_chunk(const SearchParams &P, QueryState &st, uint32_t need,
+                                  uint32_t *base, uint32_t *size) {
+  uint2 *list = P.chunks + (size_t)blockIdx.x * P.max_chunks;
+  while (st.cur_chunk + 1 < st.n_chunks) {  // a kept chunk that is large enough
+    const uint2 ch = list[++st.cur_chunk];
+    if (ch.y >= need) {
+      *base = ch.x;
+      *size = ch.y;
+      return true;
+    }
+  }
+  if ((int)st.n_chunks >= P.max_chunks) {
+    fail_query(st, VINE_ERR_CAPACITY, kSiteChunks);
+    return false;
+  }
+  const uint64_t sz = need > P.chunk ? need : P.chunk;
+  const unsigned long long b = atomicAdd(P.pool_top, (unsigned long long)sz);
+  if (b + sz > (unsigned long long)P.pool_cap) {
+    fail_query(st, VINE_ERR_CAPACITY, kSiteArena);
+    return false;
+  }
+  list[st.n_chunks] = make_uint2((uint32_t)b, (uint32_t)sz);
+  st.cur_chunk = st.n_chunks++;
+  *base = (uint32_t)b;
+  *size = (uint32_t)sz;
+  return true;
+}
 
 // Makes sure the current arena chunk has room for `need` more labels (one
 // thread, between barriers).  A batch worker keeps the chunks it was given in
@@ -187,31 +235,57 @@ enum AbortSite {
 // out at the end of each query), so the arena holds one query per worker.
 __device__ inline void pool_reserve(const SearchParams &P, QueryState &st, uint32_t need) {
   if ((uint64_t)st.chunk_fill + need <= (uint64_t)st.chunk_end) return;
-  uint2 *list = P.chunks + (size_t)blockIdx.x * P.max_chunks;
-  while (st.cur_chunk + 1 < st.n_chunks) {  // a kept chunk that is large enough
-    const uint2 ch = list[++st.cur_chunk];
-    if (ch.y >= need) {
-      st.chunk_fill = ch.x;
-      st.chunk_end = ch.x + ch.y;
-      return;
+  uint32_t base = 0, size = 0;
+  if (!next_chunk(P, st, need, &base, &size)) {
+    st.chunk_fill = st.chunk_end = 0;
+    return;
+  }
+  st.chunk_fill = base;
+  st.chunk_end = base + size;
+}
+
+// Reserves `need` consecutive arena slots while other warps of the block do
+// the same (async mode): a compare-and-swap on the (fill, end) word of the
+// current chunk; the one warp that finds the chunk exhausted moves the worker
+// to its next chunk under the chunk lock.  Returns the first slot, or kBadIdx
+// when the query failed.
+__device__ inline uint32_t arena_take(const SearchParams &P, QueryState &st, uint32_t need) {
+  unsigned long long *pk = reinterpret_cast<unsigned long long *>(&st.chunk_fill);
+  for (int it = 0; it < (1 << 20); ++it) {
+    if (*reinterpret_cast<volatile int *>(&st.abort)) return kBadIdx;
+    const unsigned long long old = *reinterpret_cast<volatile unsigned long long *>(pk);
+    const uint32_t fill = (uint32_t)old, end = (uint32_t)(old >> 32);
+    if ((uint64_t)fill + need <= (uint64_t)end) {
+      if (atomicCAS(pk, old, old + need) == old) return fill;
+      continue;
     }
+    uint32_t got = kBadIdx;
+    bool retry = false;
+    const bool locked = with_lock(&st.chunk_lock, [&]() {
+      const unsigned long long cur = *reinterpret_cast<volatile unsigned long long *>(pk);
+      if ((uint64_t)(uint32_t)cur + need <= (uint64_t)(uint32_t)(cur >> 32)) {
+        retry = true;  // another warp switched chunks meanwhile
+        return;
+      }
+      uint32_t base = 0, size = 0;
+      if (!next_chunk(P, st, need, &base, &size)) return;
+      atomicExch(pk, ((unsigned long long)(base + size) << 32) | (unsigned long long)(base + need));
+      got = base;
+    });
+    if (!locked) {
+      fail_query(st, VINE_ERR_TIMEOUT, kSiteLock);
+      return kBadIdx;
+    }
+    if (!retry) return got;
   }
-  if ((int)st.n_chunks >= P.max_chunks) {
-    fail_query(st, VINE_ERR_CAPACITY, kSiteChunks);
-    st.chunk_fill = st.chunk_end = 0;
-    return;
-  }
-  const uint64_t size = need > P.chunk ? need : P.chunk;
-  const unsigned long long base = atomicAdd(P.pool_top, (unsigned long long)size);
-  if (base + size > (unsigned long long)P.pool_cap) {
-    fail_query(st, VINE_ERR_CAPACITY, kSiteArena);
-    st.chunk_fill = st.chunk_end = 0;
-    return;
-  }
-  list[st.n_chunks] = make_uint2((uint32_t)base, (uint32_t)size);
-  st.cur_chunk = st.n_chunks++;
-  st.chunk_fill = (uint32_t)base;
-  st.chunk_end = (uint32_t)(base + size);
+  fail_query(st, VINE_ERR_TIMEOUT, kSiteArena);
+  return kBadIdx;
+}
+
+__device__ __forceinline__ uint32_t Ctx::alloc_one() {
+  if (slab_fill) return atomicAdd(slab_fill, 1u);
+  const uint32_t i = atomicAdd(&st.chunk_fill, 1u);
+  return i < *reinterpret_cast<volatile uint32_t *>(&st.chunk_end) ? i : kBadIdx;
 }
 
 // Rewinds the worker's arena to its first kept chunk (start of a query).
@@ -252,8 +326,8 @@ __device__ inline void copy_out_path(const SearchParams &P, QueryState &st, int 
 __device__ __forceinline__ void sink_improve(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent,
                              uint64_t key) {
   QueryState &st = c.st;
-  const uint32_t idx = atomicAdd(&st.chunk_fill, 1u);
-  if (idx >= st.chunk_end) {
+  const uint32_t idx = c.alloc_one();
+  if (idx == kBadIdx) {
     fail_query(st, VINE_ERR_CAPACITY, kSiteArenaAlloc);
     return;
   }
@@ -294,9 +368,11 @@ __device__ __forceinline__ void push_far(Ctx &c, const Label &l, float f) {
 
 // Offers one label (v, nd, ndl) to the search, given v's state view s.
 // from_far = true when it comes from the far pile (budget already checked);
-// returns true when a far label must stay in the far pile.
+// returns true when a far label must stay in the far pile.  A label accepted
+// into the open bucket is queued on the near ring, or, when near_out is given,
+// its arena index is returned there for the caller to queue.
 __device__ __forceinline__ bool offer_with(Ctx &c, int32_t v, float nd, float ndl, uint32_t parent,
-                                  bool from_far, const VView &s) {
+                                  bool from_far, const VView &s, uint32_t *near_out = nullptr) {
   const SearchParams &P = c.P;
   QueryState &st = c.st;
   if (!s.reach) return false;  // no feasible completion from v (bounds mode)
@@ -322,12 +398,9 @@ __device__ __forceinline__ bool offer_with(Ctx &c, int32_t v, float nd, float nd
     uint32_t idx = 0;
     bool spilled = false;
     Label *pool = P.pool;
-    uint32_t *fill = &st.chunk_fill;
-    const uint32_t end = st.chunk_end;
-    auto alloc = [pool, fill, end, v, nd, ndl, parent]() -> uint32_t {
-      const uint32_t i = atomicAdd(fill, 1u);
-      if (i >= end) return kBadIdx;
-      pool[i] = Label{v, nd, ndl, (int32_t)parent};
+    auto alloc = [&c, pool, v, nd, ndl, parent]() -> uint32_t {
+      const uint32_t i = c.alloc_one();
+      if (i != kBadIdx) pool[i] = Label{v, nd, ndl, (int32_t)parent};
       return i;
     };
     const InsertResult r =
@@ -343,12 +416,16 @@ __device__ __forceinline__ bool offer_with(Ctx &c, int32_t v, float nd, float nd
     }
     c.c_near++;
     if (spilled) c.c_spills++;
-    const uint32_t pos = atomicAdd(&st.near_tail, 1u);
-    if (pos - *reinterpret_cast<volatile uint32_t *>(&st.near_head) > P.near_mask) {
-      fail_query(st, VINE_ERR_CAPACITY, kSiteNear);  // the open bucket outgrew the ring
-      return false;
+    if (near_out) {
+      *near_out = idx;
+    } else {
+      const uint32_t pos = warp_agg_inc(&st.near_tail);
+      if (pos - *reinterpret_cast<volatile uint32_t *>(&st.near_head) > P.near_mask) {
+        fail_query(st, VINE_ERR_CAPACITY, kSiteNear);  // the open bucket outgrew the ring
+        return false;
+      }
+      c.near_ring()[pos & P.near_mask] = make_uint2(idx, (uint32_t)v);
     }
-    c.nearq[pos & P.near_mask] = idx;
     if (P.mode == VINE_MODE_PARETO && v == st.dst) {
       const uint32_t k = atomicAdd(&st.sink_n, 1u);
       if (k < (uint32_t)P.sink_cap) c.sinks[k] = idx;
@@ -378,16 +455,17 @@ __device__ __forceinline__ void expand_block(Ctx &c, const RoundBuf &rb, uint32_
   const SearchParams &P = c.P;
   QueryState &st = c.st;
   const int tid = threadIdx.x, G = blockDim.x;
+  const int sid = spread_index(tid, G);
   const float hi = bucket_hi(st);
   const long long t_load = clock64();
-  for (int i0 = tid; i0 < n; i0 += G * kBatch) {
+  for (int i0 = sid; i0 < n; i0 += G * kBatch) {
     uint32_t idx[kBatch];
     Label lab[kBatch];
     VView s[kBatch];
 #pragma unroll
     for (int b = 0; b < kBatch; ++b) {
       const int i = i0 + b * G;
-      idx[b] = i < n ? c.nearq[(first + (uint32_t)i) & P.near_mask] : 0u;
+      idx[b] = i < n ? c.near_ring()[(first + (uint32_t)i) & P.near_mask].x : 0u;
     }
 #pragma unroll
     for (int b = 0; b < kBatch; ++b)
@@ -439,7 +517,7 @@ __device__ __forceinline__ void expand_block(Ctx &c, const RoundBuf &rb, uint32_
   }
   const long long t_relax = clock64();
   if (tid == 0 && !P.grid_scope) st.load_cycles += t_relax - t_load;
-  for (int e0 = tid; e0 < total; e0 += G * kBatch) {
+  for (int e0 = sid; e0 < total; e0 += G * kBatch) {
     int vv[kBatch];
     float nd[kBatch], nl[kBatch];
     uint32_t par[kBatch];
@@ -479,7 +557,8 @@ __device__ inline void reverse_expand_block(Ctx &c, const RoundBuf &rb, int whic
   const SearchParams &P = c.P;
   QueryState &st = c.st;
   const int tid = threadIdx.x, G = blockDim.x;
-  for (int i = tid; i < n; i += G) {
+  const int sid = spread_index(tid, G);
+  for (int i = sid; i < n; i += G) {
     const int v = (int)c.nearq[(first + (uint32_t)i) & P.near_mask];
     const int beg = __ldg(&P.g.rrow[v]);
     const VView s = view_vs(&c.vs[v], st.epoch, st.qbase, st.bcur, true);
@@ -496,7 +575,7 @@ __device__ inline void reverse_expand_block(Ctx &c, const RoundBuf &rb, int whic
   const bool use_ring = ring_ok && (*reinterpret_cast<volatile uint32_t *>(&st.near_tail) -
                                     *reinterpret_cast<volatile uint32_t *>(&st.near_head)) +
                                            (uint32_t)total < P.near_mask;
-  for (int e = tid; e < total; e += G) {
+  for (int e = sid; e < total; e += G) {
     const int k = upper_index(rb.off, n, e);
     const int j = rb.beg[k] + (e - rb.off[k]);
     const int u = __ldg(&P.g.rcol[j]);
@@ -517,7 +596,7 @@ __device__ inline void reverse_expand_block(Ctx &c, const RoundBuf &rb, int whic
     }
     if (!improved) continue;
     if (nd < hi && use_ring) {
-      const uint32_t pos = atomicAdd(&st.near_tail, 1u);
+      const uint32_t pos = warp_agg_inc(&st.near_tail);
       c.nearq[pos & P.near_mask] = (uint32_t)u;
     } else {
       const uint32_t pos = warp_agg_inc(&st.far_n);
