@@ -157,13 +157,20 @@ def algorithmic_bytes(work: dict) -> float:
     return float(forward + bounds)
 
 
-def engine_config(v, policy: str, mlp, width: float):
-    base = dict(use_bounds=1, bucket_width=width, block_threads=512, table_log2=12)
+def engine_config(v, policy: str, mlp, mean_len: float):
+    """Batch-engine settings: those the scheduler network was trained with
+    (its metadata), else the scheduler module's defaults."""
+    from vine_b200 import scheduler as S
+    meta = {}
+    if policy == "mlp" and S.MODEL_JSON.exists():
+        meta = json.loads(S.MODEL_JSON.read_text())
+    kw = dict(policy=policy,
+              bucket_width=float(meta.get("base_mult", S.BASE_MULT)) * mean_len,
+              table_log2=int(meta.get("table_log2", S.TABLE_LOG2)),
+              block_threads=int(meta.get("block_threads", 512)))
     if policy == "mlp" and mlp is not None:
-        return v.Config(policy="mlp", mlp=mlp, **base)
-    if policy == "fixed":
-        return v.Config(policy="fixed", **base)
-    return v.Config(policy="ar", **base)
+        kw["mlp"] = mlp
+    return S.base_config(mean_len, **kw)
 
 
 CPU_CAP_S = 8.0  # per-query wall-time cap of the CPU reference samples
@@ -269,13 +276,13 @@ def run_vine(args):
         policy = "mlp"
     elif policy in ("auto", "mlp"):
         policy = "ar"
-    width0 = float(0.1 * w.len.mean())
-    cfg = engine_config(v, policy, mlp, width0)
+    mean_len = float(w.len.mean())
+    cfg = engine_config(v, policy, mlp, mean_len)
     tuned = ROOT / "vine_b200" / "models" / "autotune_road264k.json"
     if tuned.exists():
         for k, val in json.loads(tuned.read_text()).items():
             setattr(cfg, k, val)
-    cfg_graph = engine_config(v, policy, mlp, width0)
+    cfg_graph = engine_config(v, policy, mlp, mean_len)
     for k in ("block_threads", "table_log2", "bucket_width", "split_threshold"):
         setattr(cfg_graph, k, getattr(cfg, k))
     cfg_graph.use_cuda_graph = 1

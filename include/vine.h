@@ -105,7 +105,11 @@ typedef struct {
   int32_t sync_rounds;     /* batch engine: 1 = block-synchronous expansion
                               rounds of at most split_threshold labels;
                               0 = warps pull labels from the bucket's queue */
-  int32_t reserved[5];
+  int32_t band_mult;       /* batch engine: near far-pile band, in bucket
+                              widths (0 = 8)                                  */
+  float ar_scale;          /* AR / MLP policies: multiplier applied to the AR
+                              rule's width (0 = 1)                            */
+  int32_t reserved[3];
 } vine_config;
 
 void vine_config_default(vine_config *cfg);

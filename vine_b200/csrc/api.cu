@@ -92,9 +92,20 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
   if (!(c.bucket_width >= 0.0f) || !std::isfinite(c.bucket_width))
     return fail(VINE_ERR_INVALID, "bucket_width must be finite and >= 0");
   if (c.max_workers < 0) return fail(VINE_ERR_INVALID, "max_workers must be >= 0");
+  if (c.band_mult == 0) c.band_mult = 8;
+  if (c.ar_scale == 0.0f) c.ar_scale = 1.0f;
+  if (!(c.ar_scale >= 1.0f / 64.0f && c.ar_scale <= 64.0f))
+    return fail(VINE_ERR_INVALID, "ar_scale in [1/64, 64]");
+  if (c.band_mult < 1 || c.band_mult > 1024) return fail(VINE_ERR_INVALID, "band_mult in [1, 1024]");
   if (c.far_capacity == 0) c.far_capacity = int64_t(1) << 20;
   if (c.far_capacity < 1024 || c.far_capacity > (int64_t(1) << 30))
     return fail(VINE_ERR_INVALID, "far_capacity out of range");
+  if (c.pool_labels == 0) {
+    // keep the arena the engine already holds (resizing it would release and
+    // rebuild the whole workspace between calls)
+    const int64_t held = c.engine == VINE_ENGINE_BATCH ? g->batch.pool_cap : g->plain.pool_cap;
+    if (held > 0) c.pool_labels = held;
+  }
   if (c.pool_labels == 0) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
@@ -489,6 +500,8 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
     r.cfg.pool_labels = std::min<int64_t>(r.cfg.pool_labels * 4, (int64_t(1) << 31) - (int64_t(1) << 20));
     r.cfg.spill_log2 = std::min(r.cfg.spill_log2 + 3, 22);
     r.cfg.ctas_per_sm = 1;
+    // one worker per overflowing query: the larger per-worker piles then fit
+    r.cfg.max_workers = (int32_t)std::min<size_t>(retry.size(), 1u << 16);
     r.cfg.trace = 0;
     VINE_TRY(resolve_config(g, &r.cfg, &r));
     todo = retry;

@@ -432,6 +432,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
       st.b_candidates = st.b_spilled = st.b_relaxed = 0;
       st.r_live = 0;
       st.width = P.width0;
+      st.ar_width = P.width0;
       st.split_cap = P.round_cap;
       for (int i = 0; i < kFeat; ++i) st.x_prev[i] = 0.0f;
       const int s = st.src, t = st.dst;
@@ -889,7 +890,7 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.far_cap = w.far_cap;
   P.rest = w.rest;
   P.rest_cap = w.rest_cap;
-  P.band_mult = 8;
+  P.band_mult = c.band_mult;
   P.chunks = w.chunks;
   P.max_chunks = w.max_chunks;
   P.path_arena = w.path_arena;
@@ -911,6 +912,7 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.policy = c.policy;
   P.use_bounds = c.use_bounds;
   P.width0 = r.width0;
+  P.ar_scale = c.ar_scale;
   P.len_scale = std::max(1.0f, g->mean_len);
   P.sync_rounds = c.sync_rounds;
   P.delta_del = std::max(1.0f, 4.0f * g->mean_delay);

@@ -71,6 +71,7 @@ struct SearchParams {
   int policy;
   int use_bounds;
   float width0;
+  float ar_scale;   // multiplier on the AR rule's width (AR and MLP policies)
   float len_scale;  // mean arc length: feature normalisation
   float delta_del;
   float delta_len;
@@ -104,6 +105,7 @@ struct __align__(16) QueryState {
   uint32_t inc_idx;
   int inc_lock;
   float lo, width;
+  float ar_width;  // the AR rule's own width state (before scaling)
   uint32_t hi_bits;  // bucket upper key (float bits)
   uint32_t qbase, bcur;
   uint32_t far_n, far_wpos, far_min_bits;
@@ -676,7 +678,7 @@ __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
       // widen by 1.5x while bucket sizes fell three times in a row ("ending
       // part"), otherwise steer the forecast size towards a quarter of the
       // shared-memory table
-      width = st.width;
+      width = st.ar_width;
       const int n = st.hist_n;
       if (n >= 4 && st.hist[n - 1] < st.hist[n - 2] && st.hist[n - 2] < st.hist[n - 3] &&
           st.hist[n - 3] < st.hist[n - 4]) {
@@ -689,6 +691,8 @@ __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
         width = (float)(width * ratio);
       }
       width = fminf(fmaxf(width, P.width0 * 0.125f), P.width0 * 64.0f);
+      st.ar_width = width;
+      width *= P.ar_scale;
     }
     st.width = width;
     st.split_cap = split;
@@ -699,7 +703,8 @@ __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
     if (lane == 0) {
       const float y0 = st.y[0], y1 = st.y[1];
       if (isfinite(y0) && isfinite(y1)) {
-        st.width = P.width0 * exp2f(fminf(fmaxf(y0, -3.0f), 6.0f));
+        // the network scales the AR rule's width for this bucket
+        st.width = st.ar_width * exp2f(fminf(fmaxf(y0, -3.0f), 3.0f));
         const float lc = fminf(fmaxf(y1, 5.0f), log2f((float)P.round_cap));
         st.split_cap = max(32, min(P.round_cap, (int)exp2f(lc)));
       }

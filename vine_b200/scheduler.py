@@ -1,22 +1,23 @@
 """Learned bucket scheduler: trace collection, training and evaluation.
 
 The batch engine chooses, at every bucket boundary of every query, the width
-of the next bucket and the split threshold (labels expanded per round).  The
-reference fixes the width from an AR forecast of bucket sizes
-(algorithm/cspp.cuh:254-284); here a 16-64-64-2 FP32 MLP may choose instead,
-evaluated by one warp inside the persistent kernel.  Its outputs only change
-the order and grouping of label expansions, so answers stay exact whatever it
-predicts (a positive width and a split >= 32 are enforced by the kernel).
+of the next bucket.  The reference sets it with an AR forecast of bucket
+sizes (algorithm/cspp.cuh:254-284): widen 1.5x while sizes fall, otherwise
+steer the forecast size to a quarter of the shared table.  Here a 16-64-64-2
+FP32 MLP, evaluated by one warp inside the persistent kernel, scales the AR
+rule's width for the next bucket by 2^y (y clamped to [-3, 3]) from 16
+frontier statistics.  It only changes how work is grouped into buckets, so
+answers stay exact whatever it predicts.
 
 Training data comes from the plain method itself: the engine runs a query set
-with the fixed policy at every width in WIDTH_MULTS x split in SPLITS, with
-tracing on.  Each trace row holds the 16 features the scheduler saw when a
-bucket was opened.  For every query the setting with the fewest SM cycles
-(VINE_STAT_CYCLES) is its label; every trace row of that query, from every
-setting, becomes one training example (features -> log2(best width / base
-width), log2(best split)).  Rows from all settings keep the network from
-learning "keep the current width" from the width feature.  Training runs on
-the GPU through libvine's own forward/backward and Adam kernels.
+under the AR policy with every global width multiplier in SCALES
+(vine_config.ar_scale), with tracing on.  Each trace row holds the 16
+features the scheduler saw when a bucket was opened.  For every query the
+multiplier with the fewest SM cycles (VINE_STAT_CYCLES) is its label; every
+trace row of that query, from every run, becomes one training example
+(features -> log2(best multiplier)).  Rows from all runs keep the network
+from reading the answer off the width feature.  Training runs on the GPU
+through libvine's own forward/backward and Adam kernels.
 
 Usage: ``python -m vine_b200.scheduler [--train-config 2] [--eval-config 5]``
 writes vine_b200/models/scheduler_mlp.npy and scheduler_mlp.json.
@@ -32,9 +33,9 @@ import numpy as np
 
 from . import api as v
 
-WIDTH_MULTS = (0.05, 0.1, 0.25, 0.5, 1.0)  # bucket width / mean arc length
-SPLITS = (256, 1024)
-BASE_MULT = 0.1                            # width0 the network's output is relative to
+SCALES = (0.35, 0.5, 0.7, 1.0, 1.4, 2.0, 2.8)  # multipliers on the AR width
+BASE_MULT = 0.3          # initial bucket width / mean arc length
+TABLE_LOG2 = 13
 MODEL_DIR = Path(__file__).resolve().parent / "models"
 MODEL_NPY = MODEL_DIR / "scheduler_mlp.npy"
 MODEL_JSON = MODEL_DIR / "scheduler_mlp.json"
@@ -44,21 +45,20 @@ STAT_CYCLES = 7  # VINE_STAT_CYCLES
 
 def base_config(mean_len: float, **kw):
     """Batch engine settings shared by every arm of the comparison."""
-    d = dict(engine="batch", use_bounds=1, block_threads=512, table_log2=12,
+    d = dict(engine="batch", use_bounds=1, block_threads=512, table_log2=TABLE_LOG2,
              bucket_width=BASE_MULT * mean_len)
     d.update(kw)
     return v.Config(**d)
 
 
 def collect(graph: v.Graph, src, dst, budget, mean_len: float):
-    """Runs every (width, split) setting with the fixed policy and tracing on.
+    """Runs the AR policy at every multiplier in SCALES with tracing on.
     Returns (cycles[setting, q], traces: list of arrays, settings)."""
-    settings = [(m, s) for m in WIDTH_MULTS for s in SPLITS]
+    settings = list(SCALES)
     cycles = np.zeros((len(settings), len(src)), np.float64)
     traces = []
-    for k, (m, s) in enumerate(settings):
-        cfg = base_config(mean_len, policy="fixed", bucket_width=m * mean_len,
-                          split_threshold=s, trace=1)
+    for k, sc in enumerate(settings):
+        cfg = base_config(mean_len, policy="ar", ar_scale=sc, trace=1)
         r = v.solve(graph, src, dst, budget, cfg, paths=False, stats=True)
         cycles[k] = r.stats[:, STAT_CYCLES]
         traces.append(v.fetch_trace(graph))
@@ -66,7 +66,9 @@ def collect(graph: v.Graph, src, dst, budget, mean_len: float):
 
 
 def make_dataset(cycles, traces, settings, rows_per_setting: int = 200000, seed: int = 0):
-    """Features of every trace row -> the best setting of that row's query."""
+    """Features of every trace row -> log2 of the best multiplier of the
+    row's query (second output: a constant split target, unused by the
+    default asynchronous expansion)."""
     best = np.argmin(cycles, axis=0)
     rng = np.random.default_rng(seed)
     xs, ys = [], []
@@ -76,10 +78,9 @@ def make_dataset(cycles, traces, settings, rows_per_setting: int = 200000, seed:
         if tr.shape[0] > rows_per_setting:
             tr = tr[rng.choice(tr.shape[0], rows_per_setting, replace=False)]
         q = tr[:, 16].astype(np.int64)
-        m = np.array([settings[b][0] for b in best[q]], np.float32)
-        s = np.array([settings[b][1] for b in best[q]], np.float32)
+        sc = np.array([settings[b] for b in best[q]], np.float32)
         xs.append(tr[:, :16])
-        ys.append(np.stack([np.log2(m / BASE_MULT), np.log2(s)], axis=1))
+        ys.append(np.stack([np.log2(sc), np.full_like(sc, 10.0)], axis=1))
     x = np.concatenate(xs).astype(np.float32)
     y = np.concatenate(ys).astype(np.float32)
     ok = np.isfinite(x).all(1) & np.isfinite(y).all(1)
@@ -155,7 +156,7 @@ def main(argv=None):
     cycles, traces, settings = collect(g, wl.src, wl.dst, wl.budget, mean_len)
     x, y = make_dataset(cycles, traces, settings)
     best = np.argmin(cycles, axis=0)
-    hist = {f"{settings[k][0]}x{settings[k][1]}": int((best == k).sum()) for k in range(len(settings))}
+    hist = {str(settings[k]): int((best == k).sum()) for k in range(len(settings))}
     mlp, loss0, loss = train(x, y, epochs=a.epochs)
     static_best = int(np.argmin(cycles.sum(1)))
     g.close()
@@ -166,10 +167,11 @@ def main(argv=None):
     ge = ev.graph()
     res = evaluate(ge, ev.src[sel], ev.dst[sel], ev.budget[sel], float(ev.len.mean()), mlp)
     ge.close()
-    meta = {"base_mult": BASE_MULT, "train_config": a.train_config, "rows": int(x.shape[0]),
+    meta = {"base_mult": BASE_MULT, "table_log2": TABLE_LOG2, "block_threads": 512,
+            "train_config": a.train_config, "rows": int(x.shape[0]),
             "loss_initial": loss0, "loss_final": loss, "epochs": a.epochs,
             "best_setting_histogram": hist,
-            "best_static_setting": list(settings[static_best]),
+            "best_static_setting": settings[static_best],
             "oracle_best_per_query_cycles": float(cycles.min(0).sum()),
             "best_static_cycles": float(cycles[static_best].sum()),
             "eval_config": a.eval_config, "eval_queries": n, "eval": res,
