@@ -1,0 +1,56 @@
+"""What the trained bucket scheduler gains over the method without it.
+
+On queries it was not trained on (the 4096-query batch on the 264k-vertex
+road graph; training used a different query set on the same kind of graph),
+the batch engine runs the same queries under the fixed-width policy, the AR
+policy (the reference's rule) and the trained network scaling the AR width.
+Work is compared as total SM cycles over the queries (independent of how the
+queries happened to share the GPU); answers must be identical in all arms.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+STAT_CYCLES = 7
+
+
+@pytest.fixture(scope="module")
+def road():
+    import vine_b200 as v
+    w = v.Workload.generate(5)
+    sel = np.linspace(0, w.nq - 1, 384).astype(np.int64)
+    g = w.graph()
+    yield w, sel, g
+    g.close()
+
+
+def _run(g, w, sel, cfg):
+    import vine_b200 as v
+    v.solve(g, w.src[sel], w.dst[sel], w.budget[sel], cfg, paths=False)  # warm-up
+    return v.solve(g, w.src[sel], w.dst[sel], w.budget[sel], cfg, paths=False, stats=True)
+
+
+def test_trained_scheduler_beats_fixed_and_matches_ar(road):
+    from vine_b200 import scheduler
+    mlp, meta = scheduler.load()
+    if mlp is None:
+        pytest.skip("no trained scheduler committed")
+    w, sel, g = road
+    mean_len = float(w.len.mean())
+    arms = {
+        "fixed": scheduler.base_config(mean_len, policy="fixed"),
+        "ar": scheduler.base_config(mean_len, policy="ar"),
+        "mlp": scheduler.base_config(mean_len, policy="mlp", mlp=mlp),
+    }
+    res = {k: _run(g, w, sel, cfg) for k, cfg in arms.items()}
+    for k, r in res.items():
+        assert (r.status == 0).all(), k
+        assert np.array_equal(r.found, res["ar"].found), k
+        assert np.array_equal(np.where(r.found == 1, r.cost, 0), np.where(res["ar"].found == 1, res["ar"].cost, 0)), k
+    cyc = {k: float(r.stats[:, STAT_CYCLES].sum()) for k, r in res.items()}
+    print(f"SM cycles over {len(sel)} held-out queries: fixed {cyc['fixed']:.3e}, "
+          f"AR {cyc['ar']:.3e}, trained {cyc['mlp']:.3e} "
+          f"(trained/fixed {cyc['mlp'] / cyc['fixed']:.3f}, trained/AR {cyc['mlp'] / cyc['ar']:.3f})")
+    assert cyc["mlp"] < 0.8 * cyc["fixed"]
+    assert cyc["mlp"] <= 1.05 * cyc["ar"]

@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   const RoundBuf rb{r_idx, r_vid, r_d, r_dl, r_beg, r_off, scan, RC};
   c.vs = P.vs + (size_t)slot * P.g.n;
   c.nearq = P.nearq + (size_t)slot * 2 * (P.near_mask + 1u);  // uint2 entries
-  c.far = P.far + (size_t)slot * P.far_cap;
+  c.far = P.far + (size_t)slot * P.far_cap * (kBins / 2);
   c.rest = P.rest + (size_t)slot * P.rest_cap;
   c.sinks = P.sinklist + (size_t)slot * P.sink_cap;
   c.bt.tv = tv;
@@ -481,7 +481,14 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
         } else {
           st.lo = sv.hlen;
           st.hi_bits = __float_as_uint(sv.hlen + P.width0);
+          st.band_lo = sv.hlen;
           st.band_hi = sv.hlen + P.width0 * (float)P.band_mult;
+          st.bin_inv = (float)kBins / (st.band_hi - st.band_lo);
+          if (!(st.bin_inv < INFINITY)) st.bin_inv = 0.0f;
+          for (int j = 0; j < kBins; ++j) {
+            st.bin_n[j] = 0;
+            st.bin_min[j] = kInfBits;
+          }
           const uint32_t s0 = group_base(st.src, P.table_log2);
           tv[s0] = st.src;
           tw[s0] = make_float2(0.0f, 0.0f);
@@ -519,23 +526,45 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
             tv[i] = kEmpty;
           }
         }
+        if (tid == 0) {
+          // band summary (scheduler features and the next bucket's key)
+          uint32_t band_n = 0, bmin = kInfBits;
+          for (int j = 0; j < kBins; ++j) {
+            const uint32_t n = min(st.bin_n[j], (uint32_t)P.bin_cap);
+            band_n += n;
+            if (n) bmin = min(bmin, st.bin_min[j]);
+          }
+          st.far_n = band_n;
+          st.far_min_bits = bmin;
+        }
         __syncthreads();
         if (tid < 32) policy_step(P, st);
         if (tid == 0) {
           st.n_buckets++;
+          if (st.n_buckets > kMaxBuckets) fail_query(st, VINE_ERR_TIMEOUT, kSiteRounds);
           st.rb_band = 0;
-          const bool band = st.far_n > 0;
-          const float fmin = __uint_as_float(band ? st.far_min_bits : st.rest_min_bits);
+          const float fmin = __uint_as_float(min(st.far_min_bits, st.rest_min_bits));
           if (st.far_n == 0 && st.rest_n == 0) {
             st.done = 1;
           } else if (P.mode == VINE_MODE_OPTIMAL && st.inc_key != ~0ull && fmin > key_d(st.inc_key)) {
             st.done = 1;
           } else {
             st.lo = fmaxf(bucket_hi(st), fmin);
-            if (!band) {  // band ran dry: the next band starts at the rest minimum
+            if (st.far_n == 0) {  // band ran dry: a new band starts at the next key
+              st.band_lo = st.lo;
               st.band_hi = st.lo + st.width * (float)P.band_mult;
               if (!(st.band_hi > st.lo)) st.band_hi = nextafterf(st.lo, INFINITY);
+              st.bin_inv = (float)kBins / (st.band_hi - st.band_lo);
+              if (!(st.bin_inv < INFINITY)) st.bin_inv = 0.0f;  // degenerate band: one bin
+              for (int j = 0; j < kBins; ++j) {
+                st.bin_n[j] = 0;
+                st.bin_min[j] = kInfBits;
+              }
               st.rb_band = 1;
+            } else if (__uint_as_float(st.rest_min_bits) < st.band_hi) {
+              st.rb_band = 1;  // labels that found their bin full wait in the rest pile
+            }
+            if (st.rb_band) {
               st.rest_min_bits = kInfBits;
               st.rest_wpos = 0;
             }
@@ -553,7 +582,8 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
         const long long t_split = clock64();
         c.bt.bcur = st.bcur;
         if (st.rb_band) {
-          // ---- rebuild the band from the rest pile (in place, tile by tile)
+          // ---- move rest-pile labels below band_hi into their bins (in
+          // ---- place, tile by tile; a label whose bin is full stays)
           const uint32_t rn = st.rest_n;
           const uint32_t rtile = (uint32_t)G * kSplitBatch;
           for (uint32_t base = 0; base < rn; base += rtile) {
@@ -574,12 +604,15 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
               if (P.mode == VINE_MODE_OPTIMAL &&
                   f[b] > key_d(*reinterpret_cast<volatile unsigned long long *>(&st.inc_key))) {
                 // beaten by the incumbent: cannot lead to a better answer
-              } else if (f[b] < st.band_hi) {
-                push_far(c, item[b], f[b]);
-              } else {
-                const uint32_t w = warp_agg_inc(&st.rest_wpos);
-                c.rest[w] = item[b];
-                atomicMin(&st.rest_min_bits, __float_as_uint(f[b]));
+              } else if (!(f[b] < st.band_hi && push_bin(c, item[b], f[b]))) {
+                if (f[b] < bucket_hi(st)) {
+                  // it belongs to the opening bucket but its bin is full
+                  fail_query(st, VINE_ERR_CAPACITY, kSiteBand);
+                } else {
+                  const uint32_t w = warp_agg_inc(&st.rest_wpos);
+                  c.rest[w] = item[b];
+                  atomicMin(&st.rest_min_bits, __float_as_uint(f[b]));
+                }
               }
             }
             __syncthreads();
@@ -591,12 +624,23 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
           __syncthreads();
         }
         if (tid == 0) {
-          st.far_min_bits = kInfBits;
-          st.far_wpos = 0;
+          // bins that can hold keys below hi are scanned, as one sequence
+          const int last = band_bin(st, bucket_hi(st));
+          uint32_t run = 0;
+          for (int j = 0; j <= last; ++j) {
+            st.bin_pre[j] = run;
+            run += min(st.bin_n[j], (uint32_t)P.bin_cap);
+            st.bin_n[j] = min(st.bin_n[j], (uint32_t)P.bin_cap);
+            st.bin_wpos[j] = 0;
+            st.bin_min[j] = kInfBits;
+          }
+          st.bin_pre[last + 1] = run;
+          st.bin_last = last;
         }
         __syncthreads();
-        // ---- split the band: labels below hi enter the bucket
-        const uint32_t fn = st.far_n;
+        // ---- split the scanned bins: labels below hi enter the bucket
+        const int last = st.bin_last;
+        const uint32_t fn = st.bin_pre[last + 1];
         const uint32_t tile = (uint32_t)G * kSplitBatch;
         for (uint32_t base = 0; base < fn; base += tile) {
           if (tid == 0) pool_reserve(P, st, tile);
@@ -604,10 +648,17 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
           if (st.abort) break;
           Label item[kSplitBatch];
           VView sv[kSplitBatch];
+          int bj[kSplitBatch];
 #pragma unroll
           for (int b = 0; b < kSplitBatch; ++b) {
             const uint32_t i = base + (uint32_t)(b * G + tid);
-            if (i < fn) item[b] = c.far[i];
+            bj[b] = 0;
+            if (i < fn) {
+              int j = 0;
+              while (j < last && st.bin_pre[j + 1] <= i) ++j;
+              bj[b] = j;
+              item[b] = c.far[(size_t)j * (size_t)P.bin_cap + (i - st.bin_pre[j])];
+            }
           }
 #pragma unroll
           for (int b = 0; b < kSplitBatch; ++b)
@@ -618,16 +669,22 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
             if (base + (uint32_t)(b * G + tid) >= fn) break;
             const Label &it = item[b];
             if (offer_with(c, it.vid, it.d, it.dl, (uint32_t)it.parent, true, sv[b])) {
-              const uint32_t w = warp_agg_inc(&st.far_wpos);
-              c.far[w] = it;
-              atomicMin(&st.far_min_bits, __float_as_uint(P.use_bounds ? it.d + sv[b].hlen : it.d));
+              // stays in its bin (compacted in place)
+              namespace cg = cooperative_groups;
+              cg::coalesced_group act = cg::coalesced_threads();
+              cg::coalesced_group grp = cg::labeled_partition(act, bj[b]);
+              uint32_t wb = 0;
+              if (grp.thread_rank() == 0) wb = atomicAdd(&st.bin_wpos[bj[b]], grp.size());
+              const uint32_t w = grp.shfl(wb, 0) + grp.thread_rank();
+              c.far[(size_t)bj[b] * (size_t)P.bin_cap + w] = it;
+              atomicMin(&st.bin_min[bj[b]], __float_as_uint(P.use_bounds ? it.d + sv[b].hlen : it.d));
             }
           }
           __syncthreads();  // the tile's arena allocations end before the next reservation
         }
         __syncthreads();
         if (tid == 0) {
-          st.far_n = st.far_wpos;
+          for (int j = 0; j <= last; ++j) st.bin_n[j] = st.bin_wpos[j];
           st.split_items += fn;
           st.split_cycles += clock64() - t_split;
         }
@@ -783,7 +840,7 @@ void BatchWorkspace::release() {
 static int ensure_batch_workspace(vine_graph *g, const Resolved &r, int32_t nq) {
   BatchWorkspace &w = g->batch;
   const vine_config &c = r.cfg;
-  const int64_t near_cap = int64_t(1) << 20;
+  const int64_t near_cap = int64_t(1) << 22;
   const int sink_cap = 4096;
   const bool same = w.slots == r.slots && w.far_cap == c.far_capacity && w.near_cap == near_cap &&
                     w.pool_cap == c.pool_labels;
@@ -793,7 +850,9 @@ static int ensure_batch_workspace(vine_graph *g, const Resolved &r, int32_t nq) 
     VINE_CUDA_TRY(cudaMalloc(&w.vs, sizeof(VState) * n * r.slots));
     VINE_CUDA_TRY(cudaMemset(w.vs, 0, sizeof(VState) * n * r.slots));
     VINE_CUDA_TRY(cudaMalloc(&w.nearq, sizeof(uint2) * (size_t)near_cap * r.slots));
-    VINE_CUDA_TRY(cudaMalloc(&w.far, sizeof(Label) * (size_t)c.far_capacity * r.slots));
+    // the forward band: kBins bins of far_capacity / 2 labels each (the
+    // reverse bound searches use the first far_capacity labels as one pile)
+    VINE_CUDA_TRY(cudaMalloc(&w.far, sizeof(Label) * (size_t)c.far_capacity * (kBins / 2) * r.slots));
     w.rest_cap = 4 * c.far_capacity;
     VINE_CUDA_TRY(cudaMalloc(&w.rest, sizeof(Label) * (size_t)w.rest_cap * r.slots));
     w.max_chunks = 4096;
@@ -915,6 +974,8 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.ar_scale = c.ar_scale;
   P.len_scale = std::max(1.0f, g->mean_len);
   P.sync_rounds = c.sync_rounds;
+  P.binned = 1;
+  P.bin_cap = c.far_capacity / 2;
   P.delta_del = std::max(1.0f, 4.0f * g->mean_delay);
   P.delta_len = std::max(1.0f, 4.0f * g->mean_len);
   P.round_cap = r.round_cap;

@@ -21,6 +21,8 @@ constexpr int kHist = kBurgMaxN;
 constexpr uint32_t kInfBits = 0x7f800000u;
 constexpr int kScanScratch = 40;
 constexpr long long kMaxRounds = 1ll << 26;  // hard progress bound per query
+constexpr int kBins = 8;                     // key bins of the band (binned mode)
+constexpr long long kMaxBuckets = 1ll << 22; // hard bound on buckets per query
 
 struct SearchParams {
   DevGraph g;
@@ -81,6 +83,8 @@ struct SearchParams {
   int probe;
   int grid_scope;  // 1: one query spread over the whole grid (plain engine)
   int sync_rounds; // batch engine: 1 = block-synchronous rounds, 0 = warps pull work
+  int binned;      // forward band kept in kBins key bins (batch engine)
+  int64_t bin_cap; // labels per bin (far_cap / kBins)
   const float *mlp;
   float *trace;
   unsigned long long *trace_top;
@@ -119,6 +123,11 @@ struct __align__(16) QueryState {
   uint32_t pending;      // labels of the open bucket not yet fully expanded
   int chunk_lock;
   uint32_t slab_fill[32], slab_end[32];  // per-warp arena slabs (async mode)
+  // band bins (binned mode): bin j holds band labels with key in
+  // [band_lo + j / bin_inv, band_lo + (j + 1) / bin_inv)
+  uint32_t bin_n[kBins], bin_min[kBins], bin_wpos[kBins], bin_pre[kBins + 1];
+  float band_lo, bin_inv;
+  int bin_last;  // last bin scanned when the open bucket started
 
   int abort;
   int done;
@@ -347,9 +356,34 @@ __device__ __forceinline__ void sink_improve(Ctx &c, int32_t v, float nd, float 
 
 // Files a label beyond the open bucket: into the band pile when its key is
 // below band_hi, else into the rest pile.
+// Bin of key f in the band (monotone in f, clamped to [0, kBins)).
+__device__ __forceinline__ int band_bin(const QueryState &st, float f) {
+  const float x = (f - st.band_lo) * st.bin_inv;
+  return x > 0.0f ? min(kBins - 1, (int)x) : 0;
+}
+
+// Files a band label (f < band_hi) into its bin; false when the bin is full.
+__device__ __forceinline__ bool push_bin(Ctx &c, const Label &l, float f) {
+  namespace cg = cooperative_groups;
+  QueryState &st = c.st;
+  const int j = band_bin(st, f);
+  cg::coalesced_group act = cg::coalesced_threads();
+  cg::coalesced_group grp = cg::labeled_partition(act, j);
+  uint32_t base = 0;
+  if (grp.thread_rank() == 0) base = atomicAdd(&st.bin_n[j], grp.size());
+  const uint32_t pos = grp.shfl(base, 0) + grp.thread_rank();
+  if (pos >= (uint64_t)c.P.bin_cap) return false;
+  c.far[(size_t)j * (size_t)c.P.bin_cap + pos] = l;
+  atomicMin(&st.bin_min[j], __float_as_uint(f));
+  return true;
+}
+
 __device__ __forceinline__ void push_far(Ctx &c, const Label &l, float f) {
   QueryState &st = c.st;
-  if (f < st.band_hi) {
+  // binned band: a full bin sends the label to the rest pile, which is
+  // rescanned when a bucket opens while its minimum lies below band_hi
+  if (c.P.binned && f < st.band_hi && push_bin(c, l, f)) return;
+  if (!c.P.binned && f < st.band_hi) {
     const uint32_t pos = warp_agg_inc(&st.far_n);
     if (pos >= (uint64_t)c.P.far_cap) {
       fail_query(st, VINE_ERR_CAPACITY, kSiteBand);
