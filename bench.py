@@ -157,6 +157,24 @@ def algorithmic_bytes(work: dict) -> float:
     return float(forward + bounds)
 
 
+def scheduler_record() -> dict:
+    """The trained scheduler's held-out evaluation (vine_b200/models)."""
+    from vine_b200 import scheduler as S
+    if not (S.MODEL_JSON.exists() and MODEL_PATH.exists()):
+        return {}
+    meta = json.loads(S.MODEL_JSON.read_text())
+    ev = meta.get("eval", {})
+    if not all(k in ev for k in ("ar", "mlp", "fixed")):
+        return {}
+    return {"mlp_faster": ev["mlp"]["ms"] < ev["ar"]["ms"],
+            "heldout_queries": meta.get("eval_queries"),
+            "mlp_vs_ar_sm_cycles": ev["mlp"]["cycles"] / ev["ar"]["cycles"],
+            "mlp_vs_ar_batch_ms": ev["mlp"]["ms"] / ev["ar"]["ms"],
+            "mlp_vs_fixed_sm_cycles": ev["mlp"]["cycles"] / ev["fixed"]["cycles"],
+            "mlp_vs_fixed_batch_ms": ev["mlp"]["ms"] / ev["fixed"]["ms"],
+            "source": "vine_b200/models/scheduler_mlp.json (held-out evaluation)"}
+
+
 def engine_config(v, policy: str, mlp, mean_len: float):
     """Batch-engine settings: those the scheduler network was trained with
     (its metadata), else the scheduler module's defaults."""
@@ -271,10 +289,15 @@ def run_vine(args):
     g = v.Graph(w.row_ptr, w.col, w.len, w.delay, device=local)
 
     policy, mlp = args.policy, None
-    if policy in ("auto", "mlp") and MODEL_PATH.exists():
+    sched = scheduler_record()
+    if policy == "auto":
+        # the trained network drives the buckets when its held-out evaluation
+        # finished the batch faster than the AR rule it refines; otherwise the
+        # AR rule (the fallback and judge) does
+        policy = "mlp" if sched.get("mlp_faster") else "ar"
+    if policy == "mlp" and MODEL_PATH.exists():
         mlp = v.MLP(device=local, params=np.load(MODEL_PATH))
-        policy = "mlp"
-    elif policy in ("auto", "mlp"):
+    elif policy == "mlp":
         policy = "ar"
     mean_len = float(w.len.mean())
     cfg = engine_config(v, policy, mlp, mean_len)
@@ -318,10 +341,13 @@ def run_vine(args):
     torch.cuda.synchronize(dev)
     status = out["status"].cpu().numpy()
     if (status != 0).any():
-        r = v.solve(g, w.src[status != 0][:64], w.dst[status != 0][:64], w.budget[status != 0][:64],
-                    cfg, paths=False, stats=True, raise_on_error=False)
-        raise SystemExit(f"rank {rank}: {(status != 0).sum()} queries failed (status "
-                         f"{np.unique(status)}; abort sites {np.unique(r.stats[:, 8])})")
+        bad = np.nonzero(status != 0)[0]
+        stats = torch.zeros((nq, v._lib.STAT_COUNT), dtype=torch.int64, device=dev)
+        v.solve_device(g, src, dst, bud, dict(out_nopath, stats=stats), cfg, stream)
+        torch.cuda.synchronize(dev)
+        raise SystemExit(f"rank {rank}: {len(bad)} queries failed (status {np.unique(status)}; "
+                         f"queries {bad[:8].tolist()}; abort sites on a rerun "
+                         f"{np.unique(stats.cpu().numpy()[bad, 8]).tolist()})")
     parity = None
     work = load_work_counts()
     if rank == 0 and work is not None and work.get("nq") == nq:
@@ -423,6 +449,7 @@ def run_vine(args):
         "clocks": clocks,
         "roofline": roof,
         "parity": parity,
+        "scheduler": sched,
     }
     if not args.no_baselines and world == 1:
         line["cpu_baseline"] = cpu_reference_sample(w)

@@ -587,6 +587,9 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
           const uint32_t rn = st.rest_n;
           const uint32_t rtile = (uint32_t)G * kSplitBatch;
           for (uint32_t base = 0; base < rn; base += rtile) {
+            if (tid == 0) pool_reserve(P, st, rtile);  // for labels offered directly
+            __syncthreads();
+            if (st.abort) break;
             Label item[kSplitBatch];
             float f[kSplitBatch];
 #pragma unroll
@@ -606,8 +609,10 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
                 // beaten by the incumbent: cannot lead to a better answer
               } else if (!(f[b] < st.band_hi && push_bin(c, item[b], f[b]))) {
                 if (f[b] < bucket_hi(st)) {
-                  // it belongs to the opening bucket but its bin is full
-                  fail_query(st, VINE_ERR_CAPACITY, kSiteBand);
+                  // it belongs to the opening bucket but its bin is full:
+                  // offer it now (a far label below hi always enters)
+                  const Label &it = item[b];
+                  offer(c, it.vid, it.d, it.dl, (uint32_t)it.parent, true);
                 } else {
                   const uint32_t w = warp_agg_inc(&st.rest_wpos);
                   c.rest[w] = item[b];

@@ -19,7 +19,9 @@ trace row of that query, from every run, becomes one training example
 from reading the answer off the width feature.  Training runs on the GPU
 through libvine's own forward/backward and Adam kernels.
 
-Usage: ``python -m vine_b200.scheduler [--train-config 2] [--eval-config 5]``
+Usage: ``python -m vine_b200.scheduler [--train-config 5] [--eval-config 5]``
+(training queries come from their own query seed, so the evaluation batch
+is held out).
 writes vine_b200/models/scheduler_mlp.npy and scheduler_mlp.json.
 """
 from __future__ import annotations
@@ -65,18 +67,31 @@ def collect(graph: v.Graph, src, dst, budget, mean_len: float):
     return cycles, traces, settings
 
 
-def make_dataset(cycles, traces, settings, rows_per_setting: int = 200000, seed: int = 0):
+def make_dataset(cycles, traces, settings, rows_per_setting: int = 200000, seed: int = 0,
+                 margin: float = 0.05):
     """Features of every trace row -> log2 of the best multiplier of the
     row's query (second output: a constant split target, unused by the
-    default asynchronous expansion)."""
+    default asynchronous expansion).  Rows are drawn with probability
+    proportional to their query's cost (cycles per row of the query), so the
+    heavy queries that decide a batch's running time dominate the fit.
+    A query keeps the AR rule's own width (multiplier 1) unless another
+    multiplier saves at least `margin` of its cycles, so the network departs
+    from the rule it refines only where that clearly pays."""
     best = np.argmin(cycles, axis=0)
+    ar = settings.index(1.0)
+    keep_ar = cycles[best, np.arange(cycles.shape[1])] > (1.0 - margin) * cycles[ar]
+    best = np.where(keep_ar, ar, best)
+    qcost = cycles.min(axis=0)
     rng = np.random.default_rng(seed)
     xs, ys = [], []
     for tr in traces:
         if tr.shape[0] == 0:
             continue
-        if tr.shape[0] > rows_per_setting:
-            tr = tr[rng.choice(tr.shape[0], rows_per_setting, replace=False)]
+        q = tr[:, 16].astype(np.int64)
+        rows_of_q = np.bincount(q, minlength=cycles.shape[1]).astype(np.float64)
+        p = qcost[q] / np.maximum(rows_of_q[q], 1.0)
+        p = p / p.sum()
+        tr = tr[rng.choice(tr.shape[0], min(rows_per_setting, 4 * tr.shape[0]), replace=True, p=p)]
         q = tr[:, 16].astype(np.int64)
         sc = np.array([settings[b] for b in best[q]], np.float32)
         xs.append(tr[:, :16])
@@ -142,7 +157,10 @@ def load(device: int = 0):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--train-config", type=int, default=2)
+    ap.add_argument("--train-config", type=int, default=5)
+    ap.add_argument("--train-queries", type=int, default=1024)
+    ap.add_argument("--train-seed", type=int, default=0x7EA1,
+                    help="query seed of the training batch (the bench batch uses the default seed)")
     ap.add_argument("--eval-config", type=int, default=5)
     ap.add_argument("--eval-queries", type=int, default=1024)
     ap.add_argument("--epochs", type=int, default=30)
@@ -150,7 +168,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
 
     t0 = time.time()
-    wl = v.Workload.generate(a.train_config)
+    over = {"n_pairs": a.train_queries, "query_seed": a.train_seed} if a.train_config == 5 else {}
+    wl = v.Workload.generate(a.train_config, **over)
     mean_len = float(wl.len.mean())
     g = wl.graph()
     cycles, traces, settings = collect(g, wl.src, wl.dst, wl.budget, mean_len)
