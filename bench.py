@@ -400,6 +400,27 @@ def run_vine(args):
     torch.cuda.synchronize(dev)
     kern_ms = float(np.mean([a.elapsed_time(b) for a, b in kern]))
 
+    # the bucket policy not chosen, on the same batch (kernel only, for the record)
+    arms = {policy: nq / (kern_ms / 1e3)}
+    other = "ar" if policy == "mlp" else ("mlp" if MODEL_PATH.exists() else None)
+    if other is not None:
+        omlp = mlp if other != "mlp" or mlp is not None else v.MLP(device=local, params=np.load(MODEL_PATH))
+        ocfg = engine_config(v, other, omlp, mean_len)
+        for k in ("pool_labels", "far_capacity", "max_workers"):
+            setattr(ocfg, k, getattr(cfg, k))
+        oms = []
+        for i in range(3):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            v.solve_device(g, src, dst, bud, out_nopath, ocfg, stream)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            if i > 0:
+                oms.append(e0.elapsed_time(e1))
+        arms[other] = nq / (float(np.mean(oms)) / 1e3)
+
     # end to end through the host API, pinned host buffers
     hs = torch.from_numpy(w.src).pin_memory().numpy()
     hd = torch.from_numpy(w.dst).pin_memory().numpy()
@@ -449,7 +470,7 @@ def run_vine(args):
         "clocks": clocks,
         "roofline": roof,
         "parity": parity,
-        "scheduler": sched,
+        "scheduler": dict(sched, kernel_queries_per_s_by_policy=arms),
     }
     if not args.no_baselines and world == 1:
         line["cpu_baseline"] = cpu_reference_sample(w)

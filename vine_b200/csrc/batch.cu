@@ -32,6 +32,8 @@ namespace vine {
 
 namespace {
 
+__device__ void reverse_bucket_async(Ctx &c, int which, float radius);
+
 // One reverse bound pass (which = 0 delay, 1 length) for the query in `c`,
 // run by the whole CTA: bucketed label correcting from the sink.
 __device__ void cta_reverse_search(Ctx &c, const RoundBuf &rb, int which, float radius,
@@ -91,6 +93,17 @@ __device__ void cta_reverse_search(Ctx &c, const RoundBuf &rb, int which, float 
         __syncthreads();
       }
       if (tid == 0) st.far_n = st.far_wpos;
+      __syncthreads();
+      continue;
+    }
+    if (!P.sync_rounds) {
+      // the whole bucket, warps pulling vertices from the ring
+      if (tid == 0) {
+        st.near_commit = st.near_tail;
+        st.pending = st.near_tail - st.near_head;
+      }
+      __syncthreads();
+      reverse_bucket_async(c, which, radius);
       __syncthreads();
       continue;
     }
@@ -327,6 +340,173 @@ __device__ __forceinline__ void bucket_async(Ctx &c) {
   atomicAdd((unsigned long long *)&st.n_inserted, (unsigned long long)(c.c_near + c.c_far));
   atomicAdd((unsigned long long *)&st.n_spills, (unsigned long long)c.c_spills);
   c.c_dominated = c.c_candidates = c.c_spills = c.c_near = c.c_far = 0;
+}
+
+// Queues the vertices whose reverse distance improved below the bucket's
+// upper key (one per flagged lane) with the ordered publication of async_push;
+// entries are vertex ids in the ring's 32-bit view.
+__device__ __forceinline__ void async_push_vertex(Ctx &c, bool is_push, int32_t u) {
+  const SearchParams &P = c.P;
+  QueryState &st = c.st;
+  const int lane = threadIdx.x & 31;
+  const unsigned nm = __ballot_sync(0xffffffffu, is_push);
+  if (nm == 0) return;
+  const uint32_t k = (uint32_t)__popc(nm);
+  uint32_t base = 0;
+  if (lane == 0) {
+    base = atomicAdd(&st.near_tail, k);
+    atomicAdd(&st.pending, k);
+  }
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (is_push) {
+    const uint32_t rank = (uint32_t)__popc(nm & ((1u << lane) - 1u));
+    c.nearq[(base + rank) & P.near_mask] = (uint32_t)u;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    __threadfence_block();
+    volatile uint32_t *cm = &st.near_commit;
+    long long polls = 0;
+    while (*cm != base) {
+      if (++polls > kAsyncPolls) {
+        fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
+        break;
+      }
+    }
+    *cm = base + k;
+  }
+  __syncwarp();
+}
+
+// One bucket [lo, hi) of a reverse bound pass (which = 0 delay, 1 length) with
+// warps pulling vertices from the ring, as bucket_async does for labels: each
+// vertex's in-arcs are relaxed with its current distance; a vertex improved
+// below hi is queued again (while the ring has room), otherwise it goes to the
+// far pile.  Distances are exact whatever the order (label correcting).
+__device__ void reverse_bucket_async(Ctx &c, int which, float radius) {
+  const SearchParams &P = c.P;
+  QueryState &st = c.st;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const float hi = bucket_hi(st);
+  const uint32_t cap = P.near_mask + 1u;
+  long long idle = 0;
+  uint32_t seen_commit = 0xffffffffu, seen_pending = 0xffffffffu;
+  for (;;) {
+    uint32_t h = 0, take = 0;
+    int stop = 0;
+    if (lane == 0) {
+      for (;;) {
+        if (*reinterpret_cast<volatile int *>(&st.abort)) {
+          stop = 1;
+          break;
+        }
+        const uint32_t cm = *reinterpret_cast<volatile uint32_t *>(&st.near_commit);
+        h = *reinterpret_cast<volatile uint32_t *>(&st.near_head);
+        if (h != cm) {
+          const uint32_t avail = cm - h;
+          take = min(32u, max(1u, (avail + (uint32_t)nw - 1u) / (uint32_t)nw));
+          if (atomicCAS(&st.near_head, h, h + take) == h) break;
+          continue;
+        }
+        const uint32_t pend = *reinterpret_cast<volatile uint32_t *>(&st.pending);
+        if (pend == 0) {
+          stop = 1;
+          break;
+        }
+        if (cm != seen_commit || pend != seen_pending) {
+          seen_commit = cm;
+          seen_pending = pend;
+          idle = 0;
+        }
+        if (++idle > kAsyncPolls) {
+          fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
+          stop = 1;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    if (__shfl_sync(FULL, stop, 0)) break;
+    h = __shfl_sync(FULL, h, 0);
+    take = __shfl_sync(FULL, take, 0);
+    __threadfence_block();  // entries below near_commit are visible
+
+    float dv = 0.0f;
+    int beg = 0, deg = 0;
+    if ((uint32_t)lane < take) {
+      const int v = (int)__ldcg(&c.nearq[(h + (uint32_t)lane) & P.near_mask]);
+      const int r0 = __ldg(&P.g.rrow[v]);
+      const int r1 = __ldg(&P.g.rrow[v + 1]);
+      dv = reverse_dist(c, which, v);
+      if (dv <= radius) {
+        beg = r0;
+        deg = r1 - r0;
+      }
+    }
+    int incl = deg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    const int excl = incl - deg;
+    if (lane == 0)
+      atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_relaxed), (unsigned long long)total);
+    for (int e0 = 0; e0 < total; e0 += 32) {
+      const int e = e0 + lane;
+      int k = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int ex = __shfl_sync(FULL, excl, (k + step) & 31);
+        if (k + step < 32 && ex <= e) k += step;
+      }
+      const int obeg = __shfl_sync(FULL, beg, k);
+      const int oex = __shfl_sync(FULL, excl, k);
+      const float odv = __shfl_sync(FULL, dv, k);
+      bool push = false;
+      int u = 0;
+      if (e < total) {
+        const int j = obeg + (e - oex);
+        u = __ldg(&P.g.rcol[j]);
+        const float2 w = __ldg(&P.g.rw[j]);
+        const float nd = odv + (which == 0 ? w.y : w.x);
+        if (nd <= radius) {
+          VState *su = &c.vs[u];
+          bool improved = false;
+          if (which == 0) {
+            bool claimed = false;
+            improved = relax_pair(&su->e_del, st.epoch, nd, &claimed);
+            if (claimed) atomicExch(reinterpret_cast<unsigned int *>(&su->hlen), kInfBits);
+          } else if (__ldcg(&su->e_del) == st.epoch) {
+            const unsigned old =
+                atomicMin(reinterpret_cast<unsigned int *>(&su->hlen), __float_as_uint(nd));
+            improved = __float_as_uint(nd) < old;
+          }
+          if (improved) {
+            // ring while it has room for every warp's pushes, else far pile
+            const uint32_t used = *reinterpret_cast<volatile uint32_t *>(&st.near_tail) -
+                                  *reinterpret_cast<volatile uint32_t *>(&st.near_head);
+            if (nd < hi && used + 2u * (uint32_t)blockDim.x < cap) {
+              push = true;
+            } else {
+              const uint32_t pos = warp_agg_inc(&st.far_n);
+              if (pos >= (uint64_t)P.far_cap) {
+                fail_query(st, VINE_ERR_CAPACITY, kSiteBand);
+              } else {
+                c.far[pos] = Label{u, nd, 0.0f, -1};
+                atomicMin(&st.far_min_bits, __float_as_uint(nd));
+              }
+            }
+          }
+        }
+      }
+      async_push_vertex(c, push, u);
+    }
+    __syncwarp();
+    if (lane == 0) atomicSub(&st.pending, take);
+  }
 }
 
 // Far-pile items per thread whose loads are issued together when a bucket

@@ -155,6 +155,17 @@ def load(device: int = 0):
     return v.MLP(device=device, params=np.load(MODEL_NPY)), meta
 
 
+def _evaluate_batch(a, mlp):
+    """Fixed / AR / network on a whole batch drawn with its own query seed."""
+    over = {"n_pairs": a.eval_queries, "query_seed": a.eval_seed} if a.eval_config == 5 else {}
+    ev = v.Workload.generate(a.eval_config, **over)
+    n = len(ev.src)
+    ge = ev.graph()
+    res = evaluate(ge, ev.src, ev.dst, ev.budget, float(ev.len.mean()), mlp)
+    ge.close()
+    return res, n
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--train-config", type=int, default=5)
@@ -162,12 +173,29 @@ def main(argv=None):
     ap.add_argument("--train-seed", type=int, default=0x7EA1,
                     help="query seed of the training batch (the bench batch uses the default seed)")
     ap.add_argument("--eval-config", type=int, default=5)
-    ap.add_argument("--eval-queries", type=int, default=1024)
+    ap.add_argument("--eval-queries", type=int, default=4096)
+    ap.add_argument("--eval-seed", type=int, default=0xE7A1,
+                    help="query seed of the evaluation batch (neither the training nor the bench batch)")
+    ap.add_argument("--eval-only", action="store_true",
+                    help="re-evaluate the committed network without training")
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--out", default=None, help="write the evaluation JSON here")
     a = ap.parse_args(argv)
 
     t0 = time.time()
+    if a.eval_only:
+        mlp, meta = load()
+        if mlp is None:
+            raise SystemExit("no trained scheduler to evaluate")
+        res, n = _evaluate_batch(a, mlp)
+        meta.update({"eval_config": a.eval_config, "eval_queries": n, "eval_seed": a.eval_seed,
+                     "eval": res})
+        MODEL_JSON.write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
+        text = json.dumps(meta, indent=1, sort_keys=True)
+        if a.out:
+            Path(a.out).write_text(text + "\n")
+        print(text)
+        return
     over = {"n_pairs": a.train_queries, "query_seed": a.train_seed} if a.train_config == 5 else {}
     wl = v.Workload.generate(a.train_config, **over)
     mean_len = float(wl.len.mean())
@@ -180,12 +208,7 @@ def main(argv=None):
     static_best = int(np.argmin(cycles.sum(1)))
     g.close()
 
-    ev = v.Workload.generate(a.eval_config)
-    n = min(a.eval_queries, len(ev.src))
-    sel = np.linspace(0, len(ev.src) - 1, n).astype(np.int64)
-    ge = ev.graph()
-    res = evaluate(ge, ev.src[sel], ev.dst[sel], ev.budget[sel], float(ev.len.mean()), mlp)
-    ge.close()
+    res, n = _evaluate_batch(a, mlp)
     meta = {"base_mult": BASE_MULT, "table_log2": TABLE_LOG2, "block_threads": 512,
             "train_config": a.train_config, "rows": int(x.shape[0]),
             "loss_initial": loss0, "loss_final": loss, "epochs": a.epochs,
@@ -193,7 +216,8 @@ def main(argv=None):
             "best_static_setting": settings[static_best],
             "oracle_best_per_query_cycles": float(cycles.min(0).sum()),
             "best_static_cycles": float(cycles[static_best].sum()),
-            "eval_config": a.eval_config, "eval_queries": n, "eval": res,
+            "eval_config": a.eval_config, "eval_queries": n, "eval_seed": a.eval_seed,
+            "eval": res,
             "seconds": time.time() - t0}
     save(mlp, meta)
     text = json.dumps(meta, indent=1, sort_keys=True)
