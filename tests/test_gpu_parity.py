@@ -141,3 +141,28 @@ def test_device_entry_matches_reference(graphs, name, use_graph):
         assert np.array_equal(r.path_offsets, host.path_offsets)
         total = int(r.path_offsets[nq])
         assert np.array_equal(r.path_vertices[:total], host.path_vertices[:total])
+
+
+def test_empty_batch(graphs):
+    import vine_b200 as v
+    fx, g = graphs("kat3")
+    res = v.solve(g, np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32))
+    assert res.rc == 0 and res.cost.shape == (0,) and res.path_offsets.shape == (1,)
+
+
+@pytest.mark.parametrize("engine", ["batch", "plain"])
+def test_repeated_queries_in_one_batch(graphs, engine):
+    """Many workers solving copies of the same queries at once agree with
+    each other and with the reference."""
+    import vine_b200 as v
+    fx, g = graphs("road_small")
+    reps = 40 if engine == "batch" else 3
+    nq = len(fx["queries"])
+    src = np.tile(np.asarray(fx["src"], np.int32), reps)
+    dst = np.tile(np.asarray(fx["dst"], np.int32), reps)
+    bud = np.tile(np.asarray(fx["budget"], np.float32), reps)
+    res = v.solve(g, src, dst, bud, v.Config(engine=engine, use_bounds=1))
+    tiled = dict(fx, src=src, dst=dst, budget=bud)
+    for k in range(reps * nq):
+        # equal-cost paths may differ between copies; each must be valid
+        check_result(tiled, res, k, fx["queries"][k % nq])

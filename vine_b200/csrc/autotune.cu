@@ -1,6 +1,6 @@
-// Autotuner for the batch engine: picks block shape (threads per query
-// worker), bucket-table size and bucket granularity (width and split
-// threshold) by timing candidates on a sample of queries with CUDA events.
+// Autotuner for the batch engine: picks the bucket-table size, the bucket
+// granularity (initial width; the far band's width in buckets) and the block
+// shape by timing candidates on a sample of queries with CUDA events.
 // The reference fixes these at compile time (BLOCK_SIZE, TABLE_SIZE, VSIZE,
 // algorithm/bucket.cuh:9-13; SearchSpace, algorithm/dominance.cuh:11) and
 // sizes its split from free memory (algorithm/cspp.cuh:43-47, 136-138).
@@ -23,11 +23,12 @@ namespace {
 struct Candidate {
   int block_threads, table_log2, split;
   float width_mult;
+  int band_mult;
 };
 
 std::string cache_key(const vine_graph *g, const vine_config &c) {
   std::ostringstream ss;
-  ss << std::hex << g->fingerprint << std::dec << " m" << c.mode << " b" << c.use_bounds << " p"
+  ss << "v2 " << std::hex << g->fingerprint << std::dec << " m" << c.mode << " b" << c.use_bounds << " p"
      << c.policy;
   return ss.str();
 }
@@ -40,8 +41,8 @@ bool cache_lookup(const char *path, const std::string &key, Candidate *out) {
     if (line.compare(0, key.size(), key) != 0 || line.size() <= key.size() || line[key.size()] != '|')
       continue;
     Candidate c;
-    if (std::sscanf(line.c_str() + key.size() + 1, "%d %d %d %f", &c.block_threads, &c.table_log2,
-                    &c.split, &c.width_mult) == 4) {
+    if (std::sscanf(line.c_str() + key.size() + 1, "%d %d %d %f %d", &c.block_threads,
+                    &c.table_log2, &c.split, &c.width_mult, &c.band_mult) == 5) {
       *out = c;
       return true;
     }
@@ -53,7 +54,7 @@ void cache_store(const char *path, const std::string &key, const Candidate &c) {
   if (!path) return;
   std::ofstream out(path, std::ios::app);
   out << key << '|' << c.block_threads << ' ' << c.table_log2 << ' ' << c.split << ' '
-      << c.width_mult << '\n';
+      << c.width_mult << ' ' << c.band_mult << '\n';
 }
 
 void apply(const Candidate &k, const vine_graph *g, vine_config *c) {
@@ -61,6 +62,7 @@ void apply(const Candidate &k, const vine_graph *g, vine_config *c) {
   c->table_log2 = k.table_log2;
   c->split_threshold = k.split;
   c->bucket_width = k.width_mult * g->mean_len;
+  c->band_mult = k.band_mult;
 }
 
 }  // namespace
@@ -104,10 +106,13 @@ extern "C" int vine_autotune(vine_graph *g, int32_t nq, const int32_t *src, cons
   cudaMemcpy(d_src, src, 4 * (size_t)nq, cudaMemcpyHostToDevice);
   cudaMemcpy(d_dst, dst, 4 * (size_t)nq, cudaMemcpyHostToDevice);
   cudaMemcpy(d_budget, budget, 4 * (size_t)nq, cudaMemcpyHostToDevice);
+  // one CTA of 512 threads per SM (smaller blocks co-resident on an SM
+  // slow each other down), table of 2^12 or 2^13 slots, initial width and
+  // band width around the values that measured best on road graphs
   std::vector<Candidate> cands;
-  for (int bt : {256, 512})
-    for (int tl : {11, 12})
-      for (float wm : {0.1f, 0.25f, 0.5f}) cands.push_back({bt, tl, 0, wm});
+  for (int tl : {12, 13})
+    for (float wm : {0.2f, 0.3f, 0.5f})
+      for (int bm : {8, 16}) cands.push_back({512, tl, 0, wm, bm});
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
