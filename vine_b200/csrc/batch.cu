@@ -517,7 +517,9 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int H = 1 << P.table_log2;
   const int NL = 1 << P.lock_log2;
-  const int RC = P.round_cap;
+  // round buffers only exist for block-synchronous rounds: in the default
+  // mode their shared memory is left to the L1 cache
+  const int RC = P.sync_rounds ? P.round_cap : 0;
   int32_t *tv = reinterpret_cast<int32_t *>(smem);
   float2 *tw = reinterpret_cast<float2 *>(tv + H);
   uint32_t *ti = reinterpret_cast<uint32_t *>(tw + H);
@@ -1099,7 +1101,8 @@ int batch_prepare(vine_graph *g, const Resolved &r, int32_t nq, cudaStream_t str
     }
   }
   w.epoch_next += (uint32_t)nq;
-  const size_t smem = batch_smem_bytes(r.cfg.table_log2, lock_log2_for(r.cfg.table_log2), r.round_cap);
+  const size_t smem = batch_smem_bytes(r.cfg.table_log2, lock_log2_for(r.cfg.table_log2),
+                                       r.cfg.sync_rounds ? r.round_cap : 0);
   VINE_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
   return VINE_OK;
@@ -1173,7 +1176,7 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.trace_top = w.counters + 3;
   P.trace_cap = w.trace_cap;
 
-  const size_t smem = batch_smem_bytes(c.table_log2, P.lock_log2, r.round_cap);
+  const size_t smem = batch_smem_bytes(c.table_log2, P.lock_log2, c.sync_rounds ? r.round_cap : 0);
   VINE_CUDA_TRY(cudaMemsetAsync(w.counters, 0, sizeof(unsigned long long) * 4, stream));
   epoch_kernel<<<1, 1, 0, stream>>>(w.counters, nq);
   if (c.order_queries) VINE_TRY(order_queries(nq, d_budget, w.order, stream));
@@ -1195,7 +1198,8 @@ int batch_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d_src
 }
 
 int batch_slots(const vine_graph *g, const vine_config &c, int round_cap, int *slots) {
-  const size_t smem = batch_smem_bytes(c.table_log2, lock_log2_for(c.table_log2), round_cap);
+  const size_t smem =
+      batch_smem_bytes(c.table_log2, lock_log2_for(c.table_log2), c.sync_rounds ? round_cap : 0);
   VINE_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
   int per_sm = 0;
