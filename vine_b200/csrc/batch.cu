@@ -3,8 +3,10 @@
 // Replaces the reference's per-query host loop RUN_CSPP
 // (algorithm/cspp.cuh:134-296), which launched expand / recheck / Thrust scan
 // / fill kernels and copied the frontier size to the host every round.  Here
-// each CTA pulls a query from a device work queue, runs the whole search with
-// block barriers only, writes the result and pulls the next query.  Per-query
+// each CTA pulls a query from a device work queue (largest budget first), runs
+// the whole search on the device, writes the result and pulls the next query.
+// Inside a bucket its warps pull labels from the bucket's queue on their own
+// (no block barrier per hop); bucket changes are block-synchronous.  Per-query
 // state lives in per-worker HBM regions (reset lazily by tags) and in shared
 // memory:
 //
@@ -14,10 +16,13 @@
 //                      lists (algorithm/bucket.cuh:80-119,
 //                      algorithm/dominance.cuh:15-153)
 //   * settled delay -- one float per vertex summarising finished buckets
-//   * near queue    -- ring of arena indices still to expand in this bucket
-//   * far pile      -- labels beyond the bucket, split into later buckets
-//                      (the reference's DOP split / recheck,
-//                      algorithm/cspp.cuh:179-216, algorithm/bucket.cuh:217-245)
+//   * near queue    -- ring of (arena index, vertex) still to expand in this
+//                      bucket, published to the warps in reservation order
+//   * far band/rest -- labels beyond the bucket: a band of 8 key bins, so that
+//                      opening a bucket scans only the bins below its key, and
+//                      a rest pile behind it (the reference's DOP split /
+//                      recheck, algorithm/cspp.cuh:179-216,
+//                      algorithm/bucket.cuh:217-245)
 //   * arena         -- every accepted label with its parent, for paths
 
 #include "engine_host.h"
