@@ -18,7 +18,7 @@
 //   * settled delay -- one float per vertex summarising finished buckets
 //   * near queue    -- ring of (arena index, vertex) still to expand in this
 //                      bucket, published to the warps in reservation order
-//   * far band/rest -- labels beyond the bucket: a band of 8 key bins, so that
+//   * far band/rest -- labels beyond the bucket: a band of 16 key bins, so that
 //                      opening a bucket scans only the bins below its key, and
 //                      a rest pile behind it (the reference's DOP split /
 //                      recheck, algorithm/cspp.cuh:179-216,
@@ -545,7 +545,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   const RoundBuf rb{r_idx, r_vid, r_d, r_dl, r_beg, r_off, scan, RC};
   c.vs = P.vs + (size_t)slot * P.g.n;
   c.nearq = P.nearq + (size_t)slot * 2 * (P.near_mask + 1u);  // uint2 entries
-  c.far = P.far + (size_t)slot * P.far_cap * (kBins / 2);
+  c.far = P.far + (size_t)slot * P.far_cap * 4;
   c.rest = P.rest + (size_t)slot * P.rest_cap;
   c.sinks = P.sinklist + (size_t)slot * P.sink_cap;
   c.bt.tv = tv;
@@ -1042,9 +1042,9 @@ static int ensure_batch_workspace(vine_graph *g, const Resolved &r, int32_t nq) 
     VINE_CUDA_TRY(cudaMalloc(&w.vs, sizeof(VState) * n * r.slots));
     VINE_CUDA_TRY(cudaMemset(w.vs, 0, sizeof(VState) * n * r.slots));
     VINE_CUDA_TRY(cudaMalloc(&w.nearq, sizeof(uint2) * (size_t)near_cap * r.slots));
-    // the forward band: kBins bins of far_capacity / 2 labels each (the
+    // the forward band: kBins bins sharing 4 x far_capacity labels (the
     // reverse bound searches use the first far_capacity labels as one pile)
-    VINE_CUDA_TRY(cudaMalloc(&w.far, sizeof(Label) * (size_t)c.far_capacity * (kBins / 2) * r.slots));
+    VINE_CUDA_TRY(cudaMalloc(&w.far, sizeof(Label) * (size_t)c.far_capacity * 4 * r.slots));
     w.rest_cap = 4 * c.far_capacity;
     VINE_CUDA_TRY(cudaMalloc(&w.rest, sizeof(Label) * (size_t)w.rest_cap * r.slots));
     w.max_chunks = 4096;
@@ -1168,7 +1168,7 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.len_scale = std::max(1.0f, g->mean_len);
   P.sync_rounds = c.sync_rounds;
   P.binned = 1;
-  P.bin_cap = c.far_capacity / 2;
+  P.bin_cap = c.far_capacity * 4 / kBins;
   P.delta_del = std::max(1.0f, 4.0f * g->mean_delay);
   P.delta_len = std::max(1.0f, 4.0f * g->mean_len);
   P.round_cap = r.round_cap;
