@@ -379,6 +379,7 @@ def run_vine(args):
     torch.cuda.synchronize(dev)
     barrier()
     clocks = sampler.stop()
+    timed_failed = int((out["status"].cpu().numpy() != 0).sum())  # last timed step
     ms = sum(a.elapsed_time(b) for a, b in evs)
     ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if dist is not None:
@@ -429,9 +430,13 @@ def run_vine(args):
     v.solve(g, hs, hd, hb, cfg, paths=True, path_capacity=path_cap)  # untimed warm-up of this path
     barrier()
     t0 = time.perf_counter()
+    call_ms = []
     for _ in range(e2e_steps):
+        tc = time.perf_counter()
         r = v.solve(g, hs, hd, hb, cfg, paths=True, path_capacity=path_cap)
+        call_ms.append(round((time.perf_counter() - tc) * 1e3, 1))
     t_e2e = time.perf_counter() - t0
+    e2e_failed = int((r.status != 0).sum())
     t_t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
     if dist is not None:
         dist.all_reduce(t_t, op=dist.ReduceOp.MAX)
@@ -466,8 +471,9 @@ def run_vine(args):
                    "bucket_width": cfg.bucket_width, "split_threshold": cfg.split_threshold,
                    "cuda_graph": True, "l2": "flushed between steps (256 MiB write)"},
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": nq * 12,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h, "ms_per_call": call_ms, "failed_queries": e2e_failed},
         "gpu_launches": 6 * args.steps,
+        "failed_queries_last_timed_step": timed_failed,
         "clocks": clocks,
         "roofline": roof,
         "parity": parity,
