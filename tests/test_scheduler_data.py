@@ -1,0 +1,39 @@
+"""Host logic of the scheduler trainer (no GPU): how trace rows become
+training examples."""
+import numpy as np
+
+
+def _traces(nq, rows_per_q, seed=0):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(3):
+        q = np.repeat(np.arange(nq), rows_per_q)
+        tr = np.zeros((q.size, 20), np.float32)
+        tr[:, :16] = rng.normal(size=(q.size, 16))
+        tr[:, 16] = q
+        out.append(tr)
+    return out
+
+
+def test_labels_follow_the_best_multiplier_with_a_margin():
+    from vine_b200 import scheduler as S
+    settings = [0.5, 1.0, 2.0]
+    # query 0: 0.5 saves 20 % -> label 0.5; query 1: 2.0 saves 2 % -> keeps 1.0
+    cycles = np.array([[80.0, 120.0], [100.0, 100.0], [130.0, 98.0]])
+    x, y = S.make_dataset(cycles, _traces(2, 50), settings, rows_per_setting=4000, seed=1)
+    assert x.shape[1] == 16 and y.shape[1] == 2
+    assert set(np.unique(y[:, 0]).tolist()) <= {np.log2(0.5), 0.0}
+    assert np.all(y[:, 1] == 10.0)
+    # rows are drawn per query in proportion to its cost (query 0: 80, query 1: 98)
+    frac0 = float(np.mean(y[:, 0] == np.log2(0.5)))
+    assert 0.35 < frac0 < 0.55
+
+
+def test_rows_with_non_finite_features_are_dropped():
+    from vine_b200 import scheduler as S
+    tr = _traces(1, 20)
+    for t in tr:
+        t[::2, 3] = np.nan
+    x, y = S.make_dataset(np.array([[1.0], [1.0], [1.0]]), tr, [0.5, 1.0, 2.0],
+                          rows_per_setting=500, seed=2)
+    assert np.isfinite(x).all() and np.isfinite(y).all() and x.shape[0] > 0

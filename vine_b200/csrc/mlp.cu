@@ -165,11 +165,18 @@ __global__ void adam_kernel(float *p, float *m, float *v, const float *g, int n,
 int fb_launch(const vine_mlp *m, const float *dX, const float *dT, const int32_t *didx, int n,
               float inv_norm, float *dgrad, float *dloss, float *dY, bool backward,
               cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    VINE_CUDA_TRY(cudaFuncSetAttribute(mlp_fb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)fb_smem_bytes()));
-    attr = true;
+  // the shared-memory opt-in is a per-device attribute: set it once per device
+  static std::mutex mu;
+  static bool attr[64] = {};
+  const int dev = m->device;
+  if (dev < 0 || dev >= 64) return fail(VINE_ERR_INVALID, "device out of range");
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!attr[dev]) {
+      VINE_CUDA_TRY(cudaFuncSetAttribute(mlp_fb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)fb_smem_bytes()));
+      attr[dev] = true;
+    }
   }
   const int ntiles = (n + kTile - 1) / kTile;
   const int grid = std::max(1, std::min(ntiles, 296));
