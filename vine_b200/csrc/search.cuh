@@ -737,8 +737,9 @@ __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
     if (lane == 0) {
       const float y0 = st.y[0], y1 = st.y[1];
       if (isfinite(y0) && isfinite(y1)) {
-        // the network scales the AR rule's width for this bucket
-        st.width = st.ar_width * exp2f(fminf(fmaxf(y0, -3.0f), 3.0f));
+        // the network scales the AR rule's width for this bucket, within the
+        // range of multipliers it was trained on (2^-1.5 .. 2^1.5)
+        st.width = st.ar_width * exp2f(fminf(fmaxf(y0, -1.5f), 1.5f));
         const float lc = fminf(fmaxf(y1, 5.0f), log2f((float)P.round_cap));
         st.split_cap = max(32, min(P.round_cap, (int)exp2f(lc)));
       }

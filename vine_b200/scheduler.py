@@ -5,7 +5,7 @@ of the next bucket.  The reference sets it with an AR forecast of bucket
 sizes (algorithm/cspp.cuh:254-284): widen 1.5x while sizes fall, otherwise
 steer the forecast size to a quarter of the shared table.  Here a 16-64-64-2
 FP32 MLP, evaluated by one warp inside the persistent kernel, scales the AR
-rule's width for the next bucket by 2^y (y clamped to [-3, 3]) from 16
+rule's width for the next bucket by 2^y (y clamped to [-1.5, 1.5]) from 16
 frontier statistics.  It only changes how work is grouped into buckets, so
 answers stay exact whatever it predicts.
 
