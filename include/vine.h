@@ -150,6 +150,9 @@ typedef struct {
   int32_t *pareto_n;      /* [nq] size of the sink Pareto set                */
   int32_t pareto_stride;
   int64_t *stats;         /* [nq*VINE_STAT_COUNT] or NULL                    */
+  int32_t retried;        /* out (vine_solve): queries solved a second time,
+                             with roomier structures, after a capacity
+                             overflow                                         */
 } vine_results;
 
 /* Solves nq queries (source src[q], sink dst[q], delay budget budget[q]) from

@@ -56,7 +56,7 @@ class vine_results(C.Structure):
         ("cost", C.c_void_p), ("delay", C.c_void_p), ("found", C.c_void_p), ("status", C.c_void_p),
         ("path_offsets", C.c_void_p), ("path", C.c_void_p), ("path_capacity", C.c_int64),
         ("pareto_d", C.c_void_p), ("pareto_delay", C.c_void_p), ("pareto_n", C.c_void_p),
-        ("pareto_stride", C.c_int32), ("stats", C.c_void_p),
+        ("pareto_stride", C.c_int32), ("stats", C.c_void_p), ("retried", C.c_int32),
     ]
 
 

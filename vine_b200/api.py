@@ -170,6 +170,7 @@ class Results:
     pareto_n: Optional[np.ndarray] = None
     stats: Optional[np.ndarray] = None
     rc: int = 0
+    retried: int = 0
 
     def path(self, q: int) -> np.ndarray:
         a, b = self.path_offsets[q], self.path_offsets[q + 1]
@@ -219,6 +220,7 @@ def solve(graph: Graph, src, dst, budget, config=None, paths: bool = True,
         return solve(graph, src, dst, budget, config, paths, pareto_stride, stats,
                      path_capacity=int(r.path_offsets[nq]), raise_on_error=raise_on_error)
     r.rc = rc
+    r.retried = int(res.retried)
     if raise_on_error:
         check(rc)
     return r

@@ -361,6 +361,7 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
   const bool want_pareto = out->pareto_d && out->pareto_delay && out->pareto_n && out->pareto_stride > 0;
   const bool want_paths = out->path_offsets != nullptr;
 
+  out->retried = 0;
   std::vector<int32_t> status((size_t)nq, VINE_OK);
   std::vector<int32_t> todo((size_t)nq);
   for (int32_t i = 0; i < nq; ++i) todo[i] = i;
@@ -494,6 +495,7 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
       if (hst[i] == VINE_ERR_CAPACITY) retry.push_back(q);
     }
     if (retry.empty() || attempt >= 1) break;
+    out->retried = (int32_t)retry.size();
     // one retry with roomier per-worker structures for the overflowing queries
     ++attempt;
     r.cfg.far_capacity = std::min<int64_t>(r.cfg.far_capacity * 8, int64_t(1) << 26);
