@@ -133,7 +133,6 @@ struct __align__(16) QueryState {
   int done;
   int split_cap;
   int hist_n;
-  int ring_ok;
   uint32_t sink_n;
   uint32_t b_labels, b_expanded, b_rounds, b_dominated, b_candidates, b_spilled, b_relaxed;
   uint32_t r_live;
