@@ -207,9 +207,14 @@ __device__ __forceinline__ void bucket_async(Ctx &c) {
           stop = 1;
           break;
         }
-        const uint32_t cm = *reinterpret_cast<volatile uint32_t *>(&st.near_commit);
+        // head first, then the commit mark: the mark only grows, so the
+        // difference cannot go negative even while other warps move the head
+        // (read the other way round, a stale mark below a newer head would
+        // wrap and hand out unpublished entries)
         h = *reinterpret_cast<volatile uint32_t *>(&st.near_head);
-        if (h != cm) {
+        __threadfence_block();
+        const uint32_t cm = *reinterpret_cast<volatile uint32_t *>(&st.near_commit);
+        if ((int32_t)(cm - h) > 0) {
           const uint32_t avail = cm - h;
           take = min(32u, max(1u, (avail + (uint32_t)nw - 1u) / (uint32_t)nw));
           if (atomicCAS(&st.near_head, h, h + take) == h) break;
@@ -406,9 +411,14 @@ __device__ void reverse_bucket_async(Ctx &c, int which, float radius) {
           stop = 1;
           break;
         }
-        const uint32_t cm = *reinterpret_cast<volatile uint32_t *>(&st.near_commit);
+        // head first, then the commit mark: the mark only grows, so the
+        // difference cannot go negative even while other warps move the head
+        // (read the other way round, a stale mark below a newer head would
+        // wrap and hand out unpublished entries)
         h = *reinterpret_cast<volatile uint32_t *>(&st.near_head);
-        if (h != cm) {
+        __threadfence_block();
+        const uint32_t cm = *reinterpret_cast<volatile uint32_t *>(&st.near_commit);
+        if ((int32_t)(cm - h) > 0) {
           const uint32_t avail = cm - h;
           take = min(32u, max(1u, (avail + (uint32_t)nw - 1u) / (uint32_t)nw));
           if (atomicCAS(&st.near_head, h, h + take) == h) break;
@@ -491,8 +501,9 @@ __device__ void reverse_bucket_async(Ctx &c, int which, float radius) {
           }
           if (improved) {
             // ring while it has room for every warp's pushes, else far pile
-            const uint32_t used = *reinterpret_cast<volatile uint32_t *>(&st.near_tail) -
-                                  *reinterpret_cast<volatile uint32_t *>(&st.near_head);
+            const uint32_t hd = *reinterpret_cast<volatile uint32_t *>(&st.near_head);
+            __threadfence_block();
+            const uint32_t used = *reinterpret_cast<volatile uint32_t *>(&st.near_tail) - hd;
             if (nd < hi && used + 2u * (uint32_t)blockDim.x < cap) {
               push = true;
             } else {
