@@ -3,8 +3,10 @@
 // in global memory).  All functions take the query state by reference; the
 // caller decides where it lives.
 //
-// Per query:  bounds passes (optional) -> bucket loop { rounds of expansion
-// until the open bucket is empty -> fold -> scheduler -> split far pile }.
+// Per query:  bounds passes (optional) -> bucket loop { expansion until the
+// open bucket is empty (block-synchronous rounds, or warps pulling labels
+// from the bucket's ring in the batch engine) -> fold -> scheduler -> open
+// the next bucket from the far band / rest pile }.
 // Exactness argument: see engine.cuh.  The reference's round structure this
 // replaces is RUN_CSPP (algorithm/cspp.cuh:173-296) with
 // ck_expand_bucket_with_filter (algorithm/bucket.cuh:15-195),
