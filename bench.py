@@ -293,7 +293,7 @@ def run_vine(args):
     if policy == "auto":
         # the trained network drives the buckets when its held-out evaluation
         # finished the batch faster than the AR rule it refines; otherwise the
-        # AR rule (the fallback and judge) does
+        # AR rule (the fallback and point of comparison) does
         policy = "mlp" if sched.get("mlp_faster") else "ar"
     if policy == "mlp" and MODEL_PATH.exists():
         mlp = v.MLP(device=local, params=np.load(MODEL_PATH))
