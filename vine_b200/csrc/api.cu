@@ -61,6 +61,63 @@ struct IoBuffers {
   }
 };
 
+// vine_solve's device buffers, kept with the graph handle and grown on demand
+// (allocating and freeing them on every call cost a device-wide sync each).
+struct IoCache {
+  IoBuffers b;
+  int64_t cap_q = 0;
+  bool stats = false;
+  size_t stride = 0;
+  int64_t path_cap = 0;
+};
+
+IoCache &io_cache(vine_graph *g) {
+  if (!g->io_cache) g->io_cache = new IoCache();
+  return *static_cast<IoCache *>(g->io_cache);
+}
+
+int io_reserve(IoCache &c, int32_t k, bool stats, size_t stride) {
+  if (k <= c.cap_q && (!stats || c.stats) && stride <= c.stride) return VINE_OK;
+  c.b.release();
+  c.cap_q = 0;
+  c.path_cap = 0;
+  const size_t cap = std::max<size_t>((size_t)k, 1024);
+  const bool want_stats = stats || c.stats;
+  const size_t want_stride = std::max(stride, c.stride);
+  IoBuffers &io = c.b;
+  if (cudaMalloc(&io.src, sizeof(int32_t) * cap) != cudaSuccess ||
+      cudaMalloc(&io.dst, sizeof(int32_t) * cap) != cudaSuccess ||
+      cudaMalloc(&io.budget, sizeof(float) * cap) != cudaSuccess ||
+      cudaMalloc(&io.cost, sizeof(float) * cap) != cudaSuccess ||
+      cudaMalloc(&io.delay, sizeof(float) * cap) != cudaSuccess ||
+      cudaMalloc(&io.found, sizeof(int32_t) * cap) != cudaSuccess ||
+      cudaMalloc(&io.status, sizeof(int32_t) * cap) != cudaSuccess ||
+      cudaMalloc(&io.offsets, sizeof(int64_t) * (cap + 1)) != cudaSuccess ||
+      (want_stats && cudaMalloc(&io.stats, sizeof(int64_t) * VINE_STAT_COUNT * cap) != cudaSuccess) ||
+      (want_stride > 0 && (cudaMalloc(&io.pareto_d, sizeof(float) * want_stride * cap) != cudaSuccess ||
+                           cudaMalloc(&io.pareto_dl, sizeof(float) * want_stride * cap) != cudaSuccess ||
+                           cudaMalloc(&io.pareto_n, sizeof(int32_t) * cap) != cudaSuccess))) {
+    c.b.release();
+    return fail(VINE_ERR_CUDA, "result allocation failed");
+  }
+  c.cap_q = (int64_t)cap;
+  c.stats = want_stats;
+  c.stride = want_stride;
+  return VINE_OK;
+}
+
+int io_reserve_path(IoCache &c, int64_t n) {
+  if (n <= c.path_cap) return VINE_OK;
+  cudaFree(c.b.path);
+  c.b.path = nullptr;
+  c.path_cap = 0;
+  const int64_t cap = n + n / 4 + 1024;
+  if (cudaMalloc(&c.b.path, sizeof(int32_t) * (size_t)cap) != cudaSuccess)
+    return fail(VINE_ERR_CUDA, "path allocation failed");
+  c.path_cap = cap;
+  return VINE_OK;
+}
+
 }  // namespace
 
 int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
@@ -244,6 +301,11 @@ void vine_graph_destroy(vine_graph *g) {
   if (g->stream) cudaStreamSynchronize(g->stream);
   g->batch.release();
   g->plain.release();
+  if (g->io_cache) {
+    static_cast<IoCache *>(g->io_cache)->b.release();
+    delete static_cast<IoCache *>(g->io_cache);
+    g->io_cache = nullptr;
+  }
   cudaFree(g->row);
   cudaFree(g->col);
   cudaFree(g->w);
@@ -378,26 +440,14 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
       hd[i] = dst[todo[i]];
       hb[i] = budget[todo[i]];
     }
-    IoBuffers io;
     auto bail = [&](int st) {
       cudaStreamSynchronize(s);
-      io.release();
       return st;
     };
     const size_t stride = want_pareto ? (size_t)out->pareto_stride : 0;
-    if (cudaMalloc(&io.src, sizeof(int32_t) * k) != cudaSuccess ||
-        cudaMalloc(&io.dst, sizeof(int32_t) * k) != cudaSuccess ||
-        cudaMalloc(&io.budget, sizeof(float) * k) != cudaSuccess ||
-        cudaMalloc(&io.cost, sizeof(float) * k) != cudaSuccess ||
-        cudaMalloc(&io.delay, sizeof(float) * k) != cudaSuccess ||
-        cudaMalloc(&io.found, sizeof(int32_t) * k) != cudaSuccess ||
-        cudaMalloc(&io.status, sizeof(int32_t) * k) != cudaSuccess ||
-        cudaMalloc(&io.offsets, sizeof(int64_t) * (k + 1)) != cudaSuccess ||
-        (out->stats && cudaMalloc(&io.stats, sizeof(int64_t) * VINE_STAT_COUNT * k) != cudaSuccess) ||
-        (want_pareto && (cudaMalloc(&io.pareto_d, sizeof(float) * stride * k) != cudaSuccess ||
-                         cudaMalloc(&io.pareto_dl, sizeof(float) * stride * k) != cudaSuccess ||
-                         cudaMalloc(&io.pareto_n, sizeof(int32_t) * k) != cudaSuccess)))
-      return bail(fail(VINE_ERR_CUDA, "result allocation failed"));
+    IoCache &cache = io_cache(g);
+    VINE_TRY(io_reserve(cache, k, out->stats != nullptr, stride));
+    IoBuffers &io = cache.b;
     if (cudaMemcpyAsync(io.src, hs.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(io.dst, hd.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(io.budget, hb.data(), sizeof(float) * k, cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -407,10 +457,10 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
     o.delay = io.delay;
     o.found = io.found;
     o.status = io.status;
-    o.stats = io.stats;
-    o.pareto_d = io.pareto_d;
-    o.pareto_delay = io.pareto_dl;
-    o.pareto_n = io.pareto_n;
+    o.stats = out->stats ? io.stats : nullptr;
+    o.pareto_d = want_pareto ? io.pareto_d : nullptr;
+    o.pareto_delay = want_pareto ? io.pareto_dl : nullptr;
+    o.pareto_n = want_pareto ? io.pareto_n : nullptr;
     o.pareto_stride = (int32_t)stride;
     PathOut paths;
     int st = run_engine(g, r, k, io.src, io.dst, io.budget, hs.data(), hd.data(), hb.data(), o, s, &paths);
@@ -424,8 +474,7 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
           cudaStreamSynchronize(s) != cudaSuccess)
         return bail(fail(VINE_ERR_CUDA, std::string("engine failed: ") + cudaGetErrorString(cudaGetLastError())));
       if (off[k] > 0) {
-        if (cudaMalloc(&io.path, sizeof(int32_t) * (size_t)off[k]) != cudaSuccess)
-          return bail(fail(VINE_ERR_CUDA, "path allocation failed"));
+        if ((st = io_reserve_path(cache, off[k])) != VINE_OK) return bail(st);
         if ((st = path_gather(paths, k, io.offsets, io.path, s)) != VINE_OK) return bail(st);
         path.resize((size_t)off[k]);
         if (cudaMemcpyAsync(path.data(), io.path, sizeof(int32_t) * (size_t)off[k], cudaMemcpyDeviceToHost, s) != cudaSuccess)
@@ -470,8 +519,6 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
         if (li >= 0 && li < k) qq = (float)todo[li];
       }
     }
-    io.release();
-
     std::vector<int32_t> retry;
     for (int32_t i = 0; i < k; ++i) {
       const int32_t q = todo[i];

@@ -94,6 +94,7 @@ struct vine_graph {
   vine::BatchWorkspace batch;
   vine::PlainWorkspace plain;
   std::vector<float> last_trace;  // host copy of the last trace
+  void *io_cache = nullptr;       // device in/out buffers of vine_solve, kept between calls
   vine::DevGraph dev() const {
     vine::DevGraph g;
     g.n = n;
