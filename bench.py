@@ -36,7 +36,6 @@ sys.path.insert(0, str(ROOT))
 METRIC = "exact CSP queries/sec, batched+learned vs plain GPU, 264k-vertex road graph"
 WORKLOAD = "road264k-4096q"
 MODEL_PATH = ROOT / "vine_b200" / "models" / "scheduler_mlp.npy"
-COUNTERS_PATH = ROOT / "vine_b200" / "models" / "c5_algorithmic_work.json"
 
 
 def parse():
@@ -224,6 +223,38 @@ def cpu_reference_sample(w, count: int = 48, cap_s: float = CPU_CAP_S, seed: int
             "cpu_seconds": busy, "wall_seconds": elapsed, "stopped": capped}
 
 
+def cpu_label_setting_sample(w, count: int = 64, seed: int = 7):
+    """For information: this project's own label-setting search (the oracle's
+    restatement with the engine's pruning rules: exact reverse bounds plus an
+    incumbent) on the host cores, on a seeded sample of the batch.  Set
+    beside the reference's exhaustive CPU search it shows how much of the
+    GPU's lead over the reference is the algorithm rather than the
+    hardware."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+    g = O.CsrGraph(w.row_ptr, w.col, w.len, w.delay)
+    rg = g.reverse()
+    threads = O.cpu_count()
+    sel = np.random.default_rng(seed).choice(w.nq, min(count, w.nq), replace=False)
+
+    def one(q):  # the ctypes calls release the GIL
+        t = int(w.dst[q])
+        hl, _, _ = O.dijkstra(rg, t, "len")
+        hd, _, _ = O.dijkstra(rg, t, "delay")
+        return O.solve_label_setting(g, int(w.src[q]), t, float(w.budget[q]), h_len=hl,
+                                     h_del=hd, use_incumbent=True)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(one, sel))
+    dt = time.perf_counter() - t0
+    return {"value": len(sel) / dt, "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": f"{len(sel)} random queries of the batch (seed {seed}), bounds + label "
+                      f"setting per query, one query per thread on {threads} threads",
+            "note": "information only: same pruning rules as the GPU engine"}
+
+
 def run_reference(args):
     """The reference arm: the reference's own CPU solver on the host cores,
     each step a seeded random slice of the batch (one query per thread, each
@@ -231,13 +262,14 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import vine_b200 as v  # generator only
     from oracle import oracle as O
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU "
                           "solver built from its sources) is missing"}))
         return
-    w = workload(0, args.nq)
+    # the same seeded workload, built by the generator copy inside
+    # oracle/_ref/libvine_ref.so: this arm loads no library of the GPU engine
+    w = O.HostWorkload(5, n_pairs=args.nq)
     g = O.CsrGraph(w.row_ptr, w.col, w.len, w.delay)
     ref = O.RefSolver(g)
     threads = O.cpu_count()
@@ -401,6 +433,32 @@ def run_vine(args):
     torch.cuda.synchronize(dev)
     kern_ms = float(np.mean([a.elapsed_time(b) for a, b in kern]))
 
+    # per-query statistics of one more (untimed) launch: latency percentiles,
+    # GPU work against the oracle's minimal work, and the split's cycle share
+    stats_t = torch.zeros((nq, v._lib.STAT_COUNT), dtype=torch.int64, device=dev)
+    v.solve_device(g, src, dst, bud, dict(out_nopath, stats=stats_t), cfg, stream)
+    torch.cuda.synchronize(dev)
+    S = stats_t.cpu().numpy()
+    start = S[:, v._lib.STAT_START_NS].astype(np.float64)
+    dur = S[:, v._lib.STAT_TIME_NS].astype(np.float64)
+    done_at = start + dur - start.min()
+    latency = {"service_ms_p50": float(np.percentile(dur, 50) / 1e6),
+               "service_ms_p99": float(np.percentile(dur, 99) / 1e6),
+               "service_ms_max": float(dur.max() / 1e6),
+               "completion_ms_p50": float(np.percentile(done_at, 50) / 1e6),
+               "completion_ms_p99": float(np.percentile(done_at, 99) / 1e6),
+               "note": "service = one query on its worker (device global timer); completion = "
+                       "from the batch's first query start to the query's end, one launch"}
+    cyc = S[:, v._lib.STAT_CYCLES].astype(np.float64).sum()
+    work_line = {"gpu_labels_expanded": int(S[:, 0].sum()), "gpu_arcs_relaxed": int(S[:, 1].sum()),
+                 "split_cycle_share": float(S[:, 12].sum() / cyc),
+                 "bound_cycle_share": float(S[:, 10].sum() / cyc),
+                 "policy_cycle_share": float(S[:, 14].sum() / cyc)}
+    if work is not None and work.get("nq") == nq:
+        work_line["waste_ratio_P"] = work_line["gpu_labels_expanded"] / work["totals"]["P"]
+        work_line["waste_ratio_R"] = work_line["gpu_arcs_relaxed"] / work["totals"]["R"]
+        work_line["oracle"] = "label setting under the same pruning rules (road264k_work.json)"
+
     # the bucket policy not chosen, on the same batch (kernel only, for the record)
     arms = {policy: nq / (kern_ms / 1e3)}
     other = "ar" if policy == "mlp" else ("mlp" if MODEL_PATH.exists() else None)
@@ -429,14 +487,18 @@ def run_vine(args):
     e2e_steps = max(2, args.steps)
     v.solve(g, hs, hd, hb, cfg, paths=True, path_capacity=path_cap)  # untimed warm-up of this path
     barrier()
-    t0 = time.perf_counter()
     call_ms, retried = [], []
     for _ in range(e2e_steps):
+        # L2 flushed before every call, as between the device-timed steps;
+        # only the call itself (copies in, solve, copies out) is timed
+        flush.zero_()
+        torch.cuda.synchronize(dev)
         tc = time.perf_counter()
         r = v.solve(g, hs, hd, hb, cfg, paths=True, path_capacity=path_cap)
-        call_ms.append(round((time.perf_counter() - tc) * 1e3, 1))
+        call_ms.append((time.perf_counter() - tc) * 1e3)
         retried.append(r.retried)
-    t_e2e = time.perf_counter() - t0
+    t_e2e = sum(call_ms) / 1e3
+    call_ms = [round(x, 1) for x in call_ms]
     e2e_failed = int((r.status != 0).sum())
     t_t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
     if dist is not None:
@@ -473,7 +535,9 @@ def run_vine(args):
                    "cuda_graph": True, "l2": "flushed between steps (256 MiB write)"},
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": nq * 12,
                 "d2h_bytes_per_step": d2h, "ms_per_call": call_ms, "failed_queries": e2e_failed,
-                "retried_after_overflow": retried},
+                "retried_after_overflow": retried, "l2": "flushed before every call"},
+        "latency": latency,
+        "work": work_line,
         "gpu_launches": 6 * args.steps,
         "failed_queries_last_timed_step": timed_failed,
         "clocks": clocks,
@@ -483,18 +547,23 @@ def run_vine(args):
     }
     if not args.no_baselines and world == 1:
         line["cpu_baseline"] = cpu_reference_sample(w)
-        # the plain engine (whole GPU, one query at a time) on a sample
+        line["cpu_label_setting"] = cpu_label_setting_sample(w)
+        # the plain engine (whole GPU, one query at a time) and the batched
+        # engine on the same seeded random sample of the batch
         k = 32
+        sel = np.sort(np.random.default_rng(31).choice(nq, k, replace=False))
         cfg_plain = v.Config(engine="plain", policy="ar", use_bounds=1)
-        v.solve(g, w.src[:4], w.dst[:4], w.budget[:4], cfg_plain, paths=False)
+        v.solve(g, w.src[sel[:4]], w.dst[sel[:4]], w.budget[sel[:4]], cfg_plain, paths=False)
         t0 = time.perf_counter()
-        rp = v.solve(g, w.src[:k], w.dst[:k], w.budget[:k], cfg_plain, paths=False)
+        rp = v.solve(g, w.src[sel], w.dst[sel], w.budget[sel], cfg_plain, paths=False)
         tp = time.perf_counter() - t0
         t0 = time.perf_counter()
-        rb = v.solve(g, w.src[:k], w.dst[:k], w.budget[:k], cfg, paths=False)
+        rb = v.solve(g, w.src[sel], w.dst[sel], w.budget[sel], cfg, paths=False)
         tb = time.perf_counter() - t0
-        line["plain_gpu"] = {"value": k / tp, "unit": "queries/s", "sample": f"first {k} queries",
+        line["plain_gpu"] = {"value": k / tp, "unit": "queries/s",
+                             "sample": f"{k} random queries of the batch (seed 31)",
                              "batched_same_sample": k / tb,
+                             "batched_vs_plain_same_sample": tp / tb,
                              "agree": bool(np.array_equal(rp.cost, rb.cost))}
     print(json.dumps(line))
     if dist is not None:

@@ -109,7 +109,16 @@ typedef struct {
                               widths (0 = 8)                                  */
   float ar_scale;          /* AR / MLP policies: multiplier applied to the AR
                               rule's width (0 = 1)                            */
-  int32_t reserved[3];
+  int32_t wait_limit;      /* every bounded device wait (lock attempts, polls
+                              of the bucket queue) gives up after this many
+                              tries and fails its query with VINE_ERR_TIMEOUT
+                              (0 = 2^26)                                      */
+  int32_t time_limit_ms;   /* per-query time limit, measured on the device's
+                              global timer (host clock for the plain engine):
+                              a query still running after it stops with
+                              VINE_ERR_TIMEOUT (0 = 600000, i.e. 10 minutes;
+                              < 0 = no limit)                                 */
+  int32_t reserved[1];
 } vine_config;
 
 void vine_config_default(vine_config *cfg);
@@ -134,7 +143,30 @@ enum vine_stat {
   VINE_STAT_POLICY_CYCLES,/* device clock cycles settling + scheduler steps  */
   VINE_STAT_LOAD_CYCLES,  /* device clock cycles loading round labels + scan */
   VINE_STAT_RELAX_CYCLES, /* device clock cycles relaxing the round's arcs   */
-  VINE_STAT_COUNT = 17
+  VINE_STAT_START_NS,     /* batch engine: device global timer (ns) when the
+                             query started on its worker                     */
+  VINE_STAT_TIME_NS,      /* batch engine: the query's duration on its worker
+                             in ns (device global timer)                     */
+  VINE_STAT_COUNT = 19
+};
+
+/* Values of stats[VINE_STAT_ABORT_SITE]: where a failed query stopped. */
+enum vine_abort_site {
+  VINE_SITE_NONE = 0,
+  VINE_SITE_ARENA = 1,       /* label arena exhausted (chunk request)         */
+  VINE_SITE_ARENA_ALLOC = 2, /* label arena exhausted (slot)                  */
+  VINE_SITE_NEAR = 3,        /* the open bucket outgrew the near ring         */
+  VINE_SITE_BAND = 4,        /* far band / bound-search pile full             */
+  VINE_SITE_REST = 5,        /* rest pile full                                */
+  VINE_SITE_SINK = 6,        /* sink label list full (Pareto mode)            */
+  VINE_SITE_LOCK = 7,        /* a lock wait reached wait_limit                */
+  VINE_SITE_ROUNDS = 8,      /* round / bucket count bound                    */
+  VINE_SITE_PATH = 9,        /* path arena full                               */
+  VINE_SITE_CHUNKS = 10,     /* arena chunk list full                         */
+  VINE_SITE_INVALID = 11,    /* query arguments out of range                  */
+  VINE_SITE_ASYNC = 12,      /* a bucket-queue wait reached wait_limit        */
+  VINE_SITE_TIME = 13,       /* time_limit_ms reached                         */
+  VINE_SITE_RING = 14        /* a queue entry failed its range check          */
 };
 
 typedef struct {

@@ -38,6 +38,7 @@
 // stay below 2^24, so every FP32 addition here is exact and order-free.
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -49,6 +50,10 @@
 namespace {
 
 const float kInf = std::numeric_limits<float>::infinity();
+
+// Optional wall-clock limit of the next label-setting searches on this thread
+// (oracle_set_time_limit); a search that passes it stops and returns 2.
+thread_local double tl_limit_s = 0.0;
 
 struct Lab {
   int vid;
@@ -320,7 +325,21 @@ int oracle_solve_label_setting(int32_t n, const int64_t *row_ptr, const int32_t 
       inc_node = 0;
     }
   }
+  const auto t_start = std::chrono::steady_clock::now();
+  int64_t pops = 0;
   while (!pq.empty()) {
+    if (tl_limit_s > 0.0 && (++pops & 4095) == 0 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count() >
+            tl_limit_s) {
+      out->found = 0;
+      out->P = c.P;
+      out->R = c.R;
+      out->S = c.S;
+      out->I = c.I;
+      out->path_len = 0;
+      out->pareto_n = 0;
+      return 2;  // stopped at the time limit: no result
+    }
     Item it = pq.top();
     pq.pop();
     const Lab lab = labs[it.lab];
@@ -378,6 +397,10 @@ int oracle_solve_label_setting(int32_t n, const int64_t *row_ptr, const int32_t 
   if (out->pareto_n > pareto_cap && pareto_d != nullptr) rc = -1;
   return rc;
 }
+
+// Sets the wall-clock limit (seconds, 0 = none) of the label-setting searches
+// that the calling thread runs next.
+void oracle_set_time_limit(double seconds) { tl_limit_s = seconds > 0.0 ? seconds : 0.0; }
 
 // Lexicographic Dijkstra over (w1, w2) from src.  dist1/dist2 receive the
 // primary distance and the secondary weight of the lexicographically shortest

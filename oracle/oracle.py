@@ -26,9 +26,15 @@ ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_SO = HERE / "_ref" / "libvine_ref.so"
 
 
-def build(ref_tree: str = "/root/reference") -> None:
+# Where the reference sources are read from when building libvine_ref.so
+# (VINE_REF_TREE overrides); machines without the tree use the prebuilt file.
+REF_TREE = os.environ.get("VINE_REF_TREE", "/root/reference")
+
+
+def build(ref_tree: str | None = None) -> None:
     """Builds liboracle.so, and libvine_ref.so when the reference tree exists."""
-    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={ref_tree}"], check=True)
+    tree = ref_tree or REF_TREE
+    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={tree}"], check=True)
 
 
 class Result(C.Structure):
@@ -60,6 +66,8 @@ def _lib_oracle():
                                                    C.c_int32, C.c_float, vp, vp, C.c_int32, vp,
                                                    C.c_int32, vp, vp, C.c_int32, C.POINTER(Result)]
         lib.oracle_dijkstra.argtypes = [C.c_int32, vp, vp, vp, vp, C.c_int32, vp, vp, vp]
+        lib.oracle_set_time_limit.argtypes = [C.c_double]
+        lib.oracle_set_time_limit.restype = None
         _oracle = lib
     return _oracle
 
@@ -82,6 +90,13 @@ def _lib_ref():
                                   vp, C.c_int32, vp, vp]
         lib.ref_solve_capped.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_double, vp,
                                          vp, vp, vp, vp]
+        lib.ref_last_error.restype = C.c_char_p
+        lib.vine_workload_default_params.argtypes = [C.c_int32, vp]
+        lib.vine_workload_generate.argtypes = [vp, C.POINTER(vp)]
+        lib.vine_workload_graph.argtypes = [vp] + [vp] * 6
+        lib.vine_workload_queries.argtypes = [vp] + [vp] * 5
+        lib.vine_workload_destroy.argtypes = [vp]
+        lib.vine_workload_destroy.restype = None
         _ref = lib
     return _ref
 
@@ -124,9 +139,12 @@ def solve_reference_rules(g: CsrGraph, src: int, dst: int, budget: float, path_c
 
 
 def solve_label_setting(g: CsrGraph, src: int, dst: int, budget: float, h_len=None, h_del=None,
-                        use_incumbent: bool = True, path_cap=None, pareto_cap: int = 4096):
-    """Label setting under the engine's pruning rules (minimal work counts)."""
+                        use_incumbent: bool = True, path_cap=None, pareto_cap: int = 4096,
+                        time_limit: float = 0.0):
+    """Label setting under the engine's pruning rules (minimal work counts).
+    With time_limit > 0 a search that runs longer returns None."""
     lib = _lib_oracle()
+    lib.oracle_set_time_limit(float(time_limit))
     cap = path_cap or g.n + 1
     path = np.zeros(cap, np.int32)
     pd = np.zeros(pareto_cap, np.float32)
@@ -137,6 +155,9 @@ def solve_label_setting(g: CsrGraph, src: int, dst: int, budget: float, h_len=No
     rc = lib.oracle_solve_label_setting(g.n, _p(g.row_ptr), _p(g.col), _p(g.len), _p(g.delay),
                                         src, dst, budget, _p(hl), _p(hd), int(use_incumbent),
                                         _p(path), cap, _p(pd), _p(pl), pareto_cap, C.byref(r))
+    lib.oracle_set_time_limit(0.0)
+    if rc == 2:
+        return None
     if rc != 0:
         raise RuntimeError("oracle buffer too small")
     return _pack(r, path, pd, pl)
@@ -231,6 +252,71 @@ class RefSolver:
             self.close()
         except Exception:
             pass
+
+
+class _WorkloadParams(C.Structure):
+    """Layout of vine_workload_params (include/vine_workloads.h)."""
+    _fields_ = [
+        ("kind", C.c_int32), ("seed", C.c_uint64), ("rows", C.c_int32), ("cols", C.c_int32),
+        ("n", C.c_int64), ("m_target", C.c_int64), ("exponent", C.c_double),
+        ("n_pairs", C.c_int32), ("n_alpha", C.c_int32), ("alpha", C.c_float * 4),
+        ("alpha_lo", C.c_float), ("alpha_hi", C.c_float), ("hop_lo", C.c_int32),
+        ("hop_hi", C.c_int32), ("hop_log_uniform", C.c_int32), ("nthreads", C.c_int32),
+        ("query_seed", C.c_uint64),
+    ]
+
+
+class HostWorkload:
+    """A seeded workload built by the generator copy inside libvine_ref.so, so
+    that CPU-only timing of the reference never loads the GPU engine's
+    library.  Same fields as vine_b200.Workload (row_ptr, col, len, delay,
+    src, dst, budget, alpha, n, m, nq); identical arrays for the same
+    parameters (checked by the tests)."""
+
+    def __init__(self, config_id: int = 1, **overrides):
+        lib = _lib_ref()
+        vp = C.c_void_p
+        p = _WorkloadParams()
+        if lib.vine_workload_default_params(config_id, C.byref(p)) != 0:
+            raise ValueError(f"bad config_id {config_id}")
+        for k, v in overrides.items():
+            if k == "alpha":
+                for i, a in enumerate(v):
+                    p.alpha[i] = a
+                p.n_alpha = len(v)
+            else:
+                setattr(p, k, v)
+        h = vp()
+        rc = lib.vine_workload_generate(C.byref(p), C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"generator failed ({rc}): {lib.ref_last_error().decode()}")
+        try:
+            n, m = C.c_int32(), C.c_int64()
+            rp, cp, lp, dp = vp(), vp(), vp(), vp()
+            lib.vine_workload_graph(h, C.byref(n), C.byref(m), C.byref(rp), C.byref(cp),
+                                    C.byref(lp), C.byref(dp))
+            self.n, self.m = n.value, m.value
+
+            def view(ptr, count, ct, dt):
+                if count == 0 or not ptr.value:
+                    return np.zeros(0, dt)
+                return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(count,)).astype(dt)
+
+            self.row_ptr = view(rp, self.n + 1, C.c_int64, np.int64)
+            self.col = view(cp, self.m, C.c_int32, np.int32)
+            self.len = view(lp, self.m, C.c_float, np.float32)
+            self.delay = view(dp, self.m, C.c_float, np.float32)
+            nq = C.c_int32()
+            sp, tp, bp, ap = vp(), vp(), vp(), vp()
+            lib.vine_workload_queries(h, C.byref(nq), C.byref(sp), C.byref(tp), C.byref(bp),
+                                      C.byref(ap))
+            self.nq = nq.value
+            self.src = view(sp, self.nq, C.c_int32, np.int32)
+            self.dst = view(tp, self.nq, C.c_int32, np.int32)
+            self.budget = view(bp, self.nq, C.c_float, np.float32)
+            self.alpha = view(ap, self.nq, C.c_float, np.float32)
+        finally:
+            lib.vine_workload_destroy(h)
 
 
 def bytes_per_query(counters: dict) -> int:

@@ -30,6 +30,7 @@
 #include <chrono>
 #include <cstdint>
 #include <limits>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -288,3 +289,15 @@ int ref_solve(void *h, int32_t nq, const int32_t *src, const int32_t *dst, const
 }
 
 }  // extern "C"
+
+// The seeded workload generator (vine_b200/csrc/workloads.cpp, compiled into
+// this library by oracle/Makefile) reports errors through vine::set_error;
+// this library keeps the text for ref_last_error().  With the generator in
+// here, the CPU reference timing builds its input without loading the GPU
+// engine's library.
+namespace vine {
+thread_local std::string g_ref_last_error;
+void set_error(const std::string &msg) { g_ref_last_error = msg; }
+}  // namespace vine
+
+extern "C" const char *ref_last_error(void) { return vine::g_ref_last_error.c_str(); }

@@ -73,3 +73,35 @@ def check_result(fx, res, q, expect, mode="optimal"):
         assert sums is not None, f"q{q}: path uses a missing arc"
         assert sums == (expect["cost"], expect["delay"]), f"q{q}: path sums {sums}"
         assert sums[1] <= fx["budget"][q], f"q{q}: path violates the budget"
+
+
+SCALE_CASES = ["tech_routers_rf", "tech_internet_as", "c4_chunglu100k", "c5_sample256",
+               "c2_road264k", "c3_road1500k"]
+
+
+def scale_fixture_path(name: str) -> Path:
+    return GOLDEN / f"scale_{name}.json"
+
+
+def load_scale(name: str, with_graph: bool = True) -> dict:
+    """A full-size fixture (tests/golden/make_scale_golden.py) plus its CSR
+    arrays and query arrays."""
+    fx = json.loads(scale_fixture_path(name).read_text())
+    if with_graph:
+        if "graph_file" in fx:
+            z = np.load(GOLDEN / fx["graph_file"])
+            fx["row_ptr"] = z["row_ptr"].astype(np.int64)
+            fx["col"] = z["col"].astype(np.int32)
+            fx["len"] = z["len"].astype(np.float32)
+            fx["delay"] = z["delay"].astype(np.float32)
+        else:
+            import vine_b200 as v
+            gen = fx["generator"]
+            w = v.Workload.generate(gen["config_id"], **gen["overrides"])
+            fx["row_ptr"], fx["col"], fx["len"], fx["delay"] = w.row_ptr, w.col, w.len, w.delay
+    q = fx["queries"]
+    fx["src"] = np.array([x["src"] for x in q], np.int32)
+    fx["dst"] = np.array([x["dst"] for x in q], np.int32)
+    fx["budget"] = np.array([x["budget"] for x in q], np.float32)
+    return fx
+

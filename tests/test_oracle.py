@@ -99,3 +99,21 @@ def test_lower_bounds_are_exact_distances(oracle_mod):
 
 def test_bytes_per_query_formula(oracle_mod):
     assert oracle_mod.bytes_per_query({"P": 1, "R": 2, "S": 3, "I": 4}) == 20 + 24 + 24 + 96
+
+
+@pytest.mark.parametrize("cid,over", [(1, {}), (2, dict(rows=30, cols=30, m_target=2500, n_pairs=12)),
+                                      (3, dict(rows=28, cols=32, m_target=2300, n_pairs=16)),
+                                      (4, dict(n=2000, m_target=30000, n_pairs=16)),
+                                      (5, dict(rows=40, cols=40, m_target=4400, n_pairs=32,
+                                               hop_lo=2, hop_hi=60))])
+def test_host_generator_copy_matches_library(oracle_mod, cid, over):
+    """The generator copy linked into the reference library (used by the CPU
+    reference timing) builds the same arrays as the engine library's."""
+    O = oracle_mod
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    import vine_b200 as v
+    a = O.HostWorkload(cid, **over)
+    b = v.Workload.generate(cid, **over)
+    for k in ("row_ptr", "col", "len", "delay", "src", "dst", "budget", "alpha"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k

@@ -89,3 +89,42 @@ def test_noalloc_rejects_sizes_beyond_the_scratch():
         assert rc == v._lib.VINE_ERR_INVALID
         assert "4096" in v._lib.lib.vine_last_error().decode()
     m.close()
+
+
+def test_noalloc_sees_new_parameters_on_a_caller_stream():
+    """set_params followed directly by the no-allocation call on a
+    non-blocking stream: the kernel must read the new parameters."""
+    import torch
+    import vine_b200 as v
+    lib = v._lib.lib
+    a, b = v.MLP(seed=5), v.MLP(seed=6)
+    x, y = _data(512, seed=12)
+    want_loss, want_grad = _alloc(lib, b, x, y)
+    s = torch.cuda.Stream()
+    a.params = b.params  # no call that synchronises in between
+    rc, loss, grad = _noalloc(lib, a, x, y, C.c_void_p(s.cuda_stream))
+    assert rc == 0
+    assert abs(loss - want_loss) <= 1e-5 * max(1.0, abs(want_loss))
+    np.testing.assert_allclose(grad, want_grad, rtol=1e-4, atol=1e-6 * float(np.abs(want_grad).max()))
+    a.close()
+    b.close()
+
+
+def test_noalloc_makes_no_device_allocation():
+    """After one warm-up call, repeated calls leave the device's free memory
+    unchanged (nothing is allocated, cached or freed per call)."""
+    import torch
+    import vine_b200 as v
+    lib = v._lib.lib
+    m = v.MLP(seed=8)
+    x, y = _data(4096, seed=13)
+    assert _noalloc(lib, m, x, y)[0] == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for n in (1, 100, 4096, 2048, 4096):
+        rc, _, _ = _noalloc(lib, m, x[:n], y[:n])
+        assert rc == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory moved by {free0 - free1} bytes"
+    m.close()

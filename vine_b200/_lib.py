@@ -33,8 +33,13 @@ ENGINE_BATCH, ENGINE_PLAIN = 0, 1
 MODE_OPTIMAL, MODE_PARETO = 0, 1
 POLICY_FIXED, POLICY_AR, POLICY_MLP = 0, 1, 2
 STAT_NAMES = ["expanded", "relaxed", "inserted", "dominated", "buckets", "rounds", "spills",
-              "cycles", "abort_site", "bound_rounds", "bound_cycles", "chain_steps"]
-STAT_COUNT = 17
+              "cycles", "abort_site", "bound_rounds", "bound_cycles", "chain_steps",
+              "split_cycles", "split_items", "policy_cycles", "load_cycles", "relax_cycles",
+              "start_ns", "time_ns"]
+STAT_COUNT = 19
+STAT_CYCLES, STAT_START_NS, STAT_TIME_NS = 7, 17, 18
+STAT_ABORT_SITE = 8
+SITE_LOCK, SITE_ASYNC, SITE_TIME, SITE_RING = 7, 12, 13, 14
 MLP_IN, MLP_HIDDEN, MLP_OUT = 16, 64, 2
 MLP_PARAMS = 64 * 16 + 64 + 64 * 64 + 64 + 2 * 64 + 2
 TRACE_COLS = 20
@@ -47,7 +52,8 @@ class vine_config(C.Structure):
         ("table_log2", C.c_int32), ("spill_log2", C.c_int32), ("bucket_width", C.c_float),
         ("split_threshold", C.c_int32), ("pool_labels", C.c_int64), ("far_capacity", C.c_int64),
         ("use_cuda_graph", C.c_int32), ("order_queries", C.c_int32), ("mlp", C.c_void_p),
-        ("trace", C.c_int32), ("max_workers", C.c_int32), ("sync_rounds", C.c_int32), ("band_mult", C.c_int32), ("ar_scale", C.c_float), ("reserved", C.c_int32 * 3),
+        ("trace", C.c_int32), ("max_workers", C.c_int32), ("sync_rounds", C.c_int32), ("band_mult", C.c_int32), ("ar_scale", C.c_float),
+        ("wait_limit", C.c_int32), ("time_limit_ms", C.c_int32), ("reserved", C.c_int32 * 1),
     ]
 
 

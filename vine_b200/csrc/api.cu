@@ -61,8 +61,12 @@ struct IoBuffers {
   }
 };
 
-// vine_solve's device buffers, kept with the graph handle and grown on demand
+// vine_solve's device buffers, kept with the graph handle between calls
 // (allocating and freeing them on every call cost a device-wide sync each).
+// They follow the calls' needs: the statistics and Pareto buffers exist only
+// while calls ask for them, and a call that needs less than a quarter of the
+// held capacity gets right-sized buffers, so one large call does not keep
+// its memory for the handle's whole life.
 struct IoCache {
   IoBuffers b;
   int64_t cap_q = 0;
@@ -77,13 +81,15 @@ IoCache &io_cache(vine_graph *g) {
 }
 
 int io_reserve(IoCache &c, int32_t k, bool stats, size_t stride) {
-  if (k <= c.cap_q && (!stats || c.stats) && stride <= c.stride) return VINE_OK;
+  const size_t cap = std::max<size_t>((size_t)k, 1024);
+  if ((size_t)k <= (size_t)c.cap_q && 4 * cap > (size_t)c.cap_q && stats == c.stats &&
+      stride == c.stride)
+    return VINE_OK;
   c.b.release();
   c.cap_q = 0;
   c.path_cap = 0;
-  const size_t cap = std::max<size_t>((size_t)k, 1024);
-  const bool want_stats = stats || c.stats;
-  const size_t want_stride = std::max(stride, c.stride);
+  const bool want_stats = stats;
+  const size_t want_stride = stride;
   IoBuffers &io = c.b;
   if (cudaMalloc(&io.src, sizeof(int32_t) * cap) != cudaSuccess ||
       cudaMalloc(&io.dst, sizeof(int32_t) * cap) != cudaSuccess ||
@@ -107,7 +113,7 @@ int io_reserve(IoCache &c, int32_t k, bool stats, size_t stride) {
 }
 
 int io_reserve_path(IoCache &c, int64_t n) {
-  if (n <= c.path_cap) return VINE_OK;
+  if (n <= c.path_cap && 4 * (n + 1024) > c.path_cap) return VINE_OK;
   cudaFree(c.b.path);
   c.b.path = nullptr;
   c.path_cap = 0;
@@ -154,6 +160,9 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
   if (!(c.ar_scale >= 1.0f / 64.0f && c.ar_scale <= 64.0f))
     return fail(VINE_ERR_INVALID, "ar_scale in [1/64, 64]");
   if (c.band_mult < 1 || c.band_mult > 1024) return fail(VINE_ERR_INVALID, "band_mult in [1, 1024]");
+  if (c.wait_limit == 0) c.wait_limit = 1 << 26;
+  if (c.wait_limit < 1) return fail(VINE_ERR_INVALID, "wait_limit must be >= 0");
+  if (c.time_limit_ms == 0) c.time_limit_ms = 600000;
   if (c.far_capacity == 0) c.far_capacity = int64_t(1) << 20;
   if (c.far_capacity < 1024 || c.far_capacity > (int64_t(1) << 30))
     return fail(VINE_ERR_INVALID, "far_capacity out of range");

@@ -71,6 +71,7 @@ __device__ void cta_reverse_search(Ctx &c, const RoundBuf &rb, int which, float 
     if (avail == 0) {
       if (st.far_n == 0) break;
       if (tid == 0) {
+        over_time(P, st);
         st.lo = fmaxf(bucket_hi(st), __uint_as_float(st.far_min_bits));
         st.hi_bits = __float_as_uint(st.lo + delta);
         st.far_min_bits = kInfBits;
@@ -119,6 +120,7 @@ __device__ void cta_reverse_search(Ctx &c, const RoundBuf &rb, int which, float 
       st.near_head += (uint32_t)n_round;
       st.n_rounds++;
       if (st.n_rounds > kMaxRounds) fail_query(st, VINE_ERR_TIMEOUT, kSiteRounds);
+      over_time(P, st);
     }
     __syncthreads();
     reverse_expand_block(c, rb, which, first, n_round, radius, bucket_hi(st), true);
@@ -147,8 +149,27 @@ __device__ void cta_reverse_search(Ctx &c, const RoundBuf &rb, int which, float 
 // `pending` counts queued labels whose expansion is not finished: children
 // are counted before their parent is uncounted, so pending == 0 with nothing
 // left to take means the bucket is finished.  Every wait is bounded.
-constexpr long long kAsyncPolls = 1ll << 26;
 constexpr uint32_t kSlab = 1024;  // arena slots a warp takes at a time
+
+// Publishes ring entries [base, base + k) once every earlier reservation is
+// published (lane 0 of the producing warp).  The wait is bounded by
+// wait_limit and ends early when the query has failed; a producer that gives
+// up publishes nothing (the query is failed, and its consumers stop at the
+// abort flag before taking entries).
+__device__ __forceinline__ void publish_entries(const SearchParams &P, QueryState &st,
+                                                uint32_t base, uint32_t k) {
+  __threadfence_block();
+  volatile uint32_t *cm = &st.near_commit;
+  long long polls = 0;
+  while (*cm != base) {
+    if (*reinterpret_cast<volatile int *>(&st.abort)) return;
+    if (++polls > P.wait_limit) {
+      fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
+      return;
+    }
+  }
+  *cm = base + k;
+}
 
 __device__ __forceinline__ void async_push(Ctx &c, bool is_near, uint32_t idx, int32_t v) {
   const SearchParams &P = c.P;
@@ -170,18 +191,7 @@ __device__ __forceinline__ void async_push(Ctx &c, bool is_near, uint32_t idx, i
     c.near_ring()[(base + rank) & P.near_mask] = make_uint2(idx, (uint32_t)v);
   }
   __syncwarp();
-  if (lane == 0) {
-    __threadfence_block();
-    volatile uint32_t *cm = &st.near_commit;
-    long long polls = 0;
-    while (*cm != base) {
-      if (++polls > kAsyncPolls) {
-        fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
-        break;
-      }
-    }
-    *cm = base + k;
-  }
+  if (lane == 0) publish_entries(P, st, base, k);
   __syncwarp();
 }
 
@@ -230,8 +240,12 @@ __device__ __forceinline__ void bucket_async(Ctx &c) {
           seen_pending = pend;
           idle = 0;
         }
-        if (++idle > kAsyncPolls) {
+        if (++idle > P.wait_limit) {
           fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
+          stop = 1;
+          break;
+        }
+        if ((idle & 1023) == 0 && over_time(P, st)) {
           stop = 1;
           break;
         }
@@ -247,8 +261,16 @@ __device__ __forceinline__ void bucket_async(Ctx &c) {
     uint32_t idx = 0;
     float d = 0.0f, dl = 0.0f;
     int beg = 0, deg = 0;
+    uint2 e = make_uint2(0u, 0u);
+    bool entry_ok = false;
     if ((uint32_t)lane < take) {
-      const uint2 e = __ldcg(&ring[(h + (uint32_t)lane) & P.near_mask]);
+      e = __ldcg(&ring[(h + (uint32_t)lane) & P.near_mask]);
+      // an entry outside the arena or the vertex range would mean a protocol
+      // slip: fail the query instead of following it
+      entry_ok = (uint64_t)e.x < (uint64_t)P.pool_cap && e.y < (uint32_t)P.g.n;
+      if (!entry_ok) fail_query(st, VINE_ERR_INTERNAL, kSiteRing);
+    }
+    if (entry_ok) {
       idx = e.x;
       const int v = (int)e.y;
       const Label lab = load_label(&P.pool[idx]);  // issued together with the loads below
@@ -373,18 +395,7 @@ __device__ __forceinline__ void async_push_vertex(Ctx &c, bool is_push, int32_t 
     c.nearq[(base + rank) & P.near_mask] = (uint32_t)u;
   }
   __syncwarp();
-  if (lane == 0) {
-    __threadfence_block();
-    volatile uint32_t *cm = &st.near_commit;
-    long long polls = 0;
-    while (*cm != base) {
-      if (++polls > kAsyncPolls) {
-        fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
-        break;
-      }
-    }
-    *cm = base + k;
-  }
+  if (lane == 0) publish_entries(P, st, base, k);
   __syncwarp();
 }
 
@@ -434,8 +445,12 @@ __device__ void reverse_bucket_async(Ctx &c, int which, float radius) {
           seen_pending = pend;
           idle = 0;
         }
-        if (++idle > kAsyncPolls) {
+        if (++idle > P.wait_limit) {
           fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
+          stop = 1;
+          break;
+        }
+        if ((idle & 1023) == 0 && over_time(P, st)) {
           stop = 1;
           break;
         }
@@ -449,8 +464,15 @@ __device__ void reverse_bucket_async(Ctx &c, int which, float radius) {
 
     float dv = 0.0f;
     int beg = 0, deg = 0;
+    int v = -1;
     if ((uint32_t)lane < take) {
-      const int v = (int)__ldcg(&c.nearq[(h + (uint32_t)lane) & P.near_mask]);
+      v = (int)__ldcg(&c.nearq[(h + (uint32_t)lane) & P.near_mask]);
+      if ((uint32_t)v >= (uint32_t)P.g.n) {
+        fail_query(st, VINE_ERR_INTERNAL, kSiteRing);  // protocol slip: stop, do not follow
+        v = -1;
+      }
+    }
+    if (v >= 0) {
       const int r0 = __ldg(&P.g.rrow[v]);
       const int r1 = __ldg(&P.g.rrow[v + 1]);
       dv = reverse_dist(c, which, v);
@@ -569,6 +591,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   c.bt.vs = c.vs;
   c.bt.next = P.next;
   c.bt.chain_steps = P.stats ? &st.n_chain_steps : nullptr;
+  c.bt.spin_limit = P.wait_limit;
 
   for (int i = tid; i < H; i += G) tv[i] = kEmpty;
   for (int i = tid; i < NL; i += G) locks[i] = 0;
@@ -594,6 +617,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
     // ------------------------------------------------------------- setup
     if (tid == 0) {
       st.t0 = clock64();
+      st.g0 = global_ns();
       st.src = P.src[q];
       st.dst = P.dst[q];
       st.budget = P.budget[q];
@@ -740,6 +764,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
         if (tid == 0) {
           st.n_buckets++;
           if (st.n_buckets > kMaxBuckets) fail_query(st, VINE_ERR_TIMEOUT, kSiteRounds);
+          over_time(P, st);
           st.rb_band = 0;
           const float fmin = __uint_as_float(min(st.far_min_bits, st.rest_min_bits));
           if (st.far_n == 0 && st.rest_n == 0) {
@@ -917,6 +942,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
         st.n_rounds++;
         st.b_rounds++;
         if (st.n_rounds > kMaxRounds) fail_query(st, VINE_ERR_TIMEOUT, kSiteRounds);
+        over_time(P, st);
       }
       expand_block(c, rb, first, n_round);  // reserves the arena after its scan
       if (tid == 0) {
@@ -993,6 +1019,8 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
         s[VINE_STAT_LOAD_CYCLES] = st.load_cycles;
         s[VINE_STAT_RELAX_CYCLES] = st.relax_cycles;
         s[VINE_STAT_CHAIN_STEPS] = (long long)st.n_chain_steps;
+        s[VINE_STAT_START_NS] = (long long)st.g0;
+        s[VINE_STAT_TIME_NS] = (long long)(global_ns() - st.g0);
       }
     }
     __syncthreads();
@@ -1187,6 +1215,8 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.lock_log2 = lock_log2_for(c.table_log2);
   P.probe = 16;
   P.grid_scope = 0;
+  P.wait_limit = c.wait_limit;
+  P.time_limit_ns = c.time_limit_ms > 0 ? (unsigned long long)c.time_limit_ms * 1000000ull : 0ull;
   P.mlp = (c.policy == VINE_POLICY_MLP && c.mlp) ? c.mlp->params : nullptr;
   P.trace = c.trace ? w.trace : nullptr;
   P.trace_top = w.counters + 3;

@@ -24,7 +24,7 @@ namespace vine {
 
 constexpr int32_t kEmpty = -1;
 constexpr uint32_t kDeadBit = 0x80000000u;
-constexpr int kSpinLimit = 1 << 26;  // bounded lock spins before giving up
+constexpr long long kDefaultWaitLimit = 1ll << 26;  // bounded waits before giving up
 
 // One accepted label in the arena.  vid's top bit marks a label killed by a
 // dominating label of the same bucket.  parent is the arena index of the label
@@ -173,7 +173,7 @@ __device__ __forceinline__ void atomic_min_float_nonneg(float *addr, float v) {
 }
 
 // Runs `body` while holding spin lock *l and returns true, or returns false
-// after kSpinLimit failed attempts.  The critical section and the release
+// after `limit` failed attempts.  The critical section and the release
 // sit inside the spin loop: a lane that took the lock finishes and releases
 // it before it can reach any reconvergence point where it might wait for a
 // lane of its own warp that is still spinning on the same lock.
@@ -181,8 +181,8 @@ __device__ __forceinline__ void atomic_min_float_nonneg(float *addr, float v) {
 // plain engine's global-memory locks); the fences must then order memory for
 // the whole device, not just the block.
 template <typename Body>
-__device__ __forceinline__ bool with_lock(int *l, Body body, bool gpu_scope = false) {
-  for (int it = 0; it < kSpinLimit; ++it) {
+__device__ __forceinline__ bool with_lock(int *l, Body body, bool gpu_scope, long long limit) {
+  for (long long it = 0; it < limit; ++it) {
     if (atomicCAS(l, 0, 1) == 0) {
       if (gpu_scope) __threadfence();
       else __threadfence_block();
@@ -293,6 +293,7 @@ struct BucketTable {
   uint32_t qbase;      // first bucket id of the query
   uint32_t bcur;       // id of the open bucket
   unsigned long long *chain_steps;  // statistics: chain labels read
+  long long spin_limit;  // lock attempts before an insert gives up
 };
 
 // Dominance test of candidate (d, dl) against one stored label; kills the
@@ -415,7 +416,7 @@ __device__ __forceinline__ InsertResult table_insert(const BucketTable &bt, Labe
   int *lk = &bt.locks[(uint32_t)v & (uint32_t)bt.lock_mask];
   InsertResult r = kLockTimeout;
   with_lock(lk, [&]() { r = table_insert_locked(bt, pool, v, d, dl, idx_alloc, out_idx, spilled); },
-            gpu_scope);
+            gpu_scope, bt.spin_limit);
   return r;
 }
 

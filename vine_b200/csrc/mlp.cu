@@ -236,9 +236,13 @@ int vine_mlp_create(int32_t device, uint64_t seed, const float *params, vine_mlp
     vine_mlp_destroy(m);
     return fail(VINE_ERR_CUDA, "parameter allocation failed");
   }
-  cudaMemcpy(m->params, p.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice);
-  cudaMemset(m->adam_m, 0, sizeof(float) * kMlpParams);
-  cudaMemset(m->adam_v, 0, sizeof(float) * kMlpParams);
+  if (cudaMemcpy(m->params, p.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(m->adam_m, 0, sizeof(float) * kMlpParams) != cudaSuccess ||
+      cudaMemset(m->adam_v, 0, sizeof(float) * kMlpParams) != cudaSuccess ||
+      cudaStreamSynchronize(0) != cudaSuccess) {  // the upload has landed before any stream uses it
+    vine_mlp_destroy(m);
+    return fail(VINE_ERR_CUDA, "parameter upload failed");
+  }
   *out = m;
   return VINE_OK;
 }
@@ -263,6 +267,9 @@ int vine_mlp_set_params(vine_mlp *m, const float *params) {
   if (!m || !params) return fail(VINE_ERR_INVALID, "bad arguments");
   VINE_CUDA_TRY(cudaSetDevice(m->device));
   VINE_CUDA_TRY(cudaMemcpy(m->params, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
+  // a copy from pageable memory may return before the DMA lands; wait for the
+  // legacy stream so a kernel on a non-blocking caller stream sees the values
+  VINE_CUDA_TRY(cudaStreamSynchronize(0));
   return VINE_OK;
 }
 
@@ -366,7 +373,8 @@ constexpr size_t kNaAlign = 64;  // floats: 256 bytes
 constexpr size_t kNaGrad = kNaAlign;
 constexpr size_t kNaX = kNaGrad + ((kMlpParams + kNaAlign - 1) / kNaAlign) * kNaAlign;
 constexpr size_t kNaT = kNaX + (size_t)kNaMaxRows * kFeat;
-constexpr size_t kNaFloats = kNaT + (size_t)kNaMaxRows * kOut;  // 79,168 floats = 309 KiB
+constexpr size_t kNaFloats = kNaT + (size_t)kNaMaxRows * kOut;  // 79,232 floats = 309.5 KiB
+static_assert(kNaFloats == 79232, "no-allocation scratch size changed: update the documented size");
 
 static __device__ __align__(256) float g_noalloc_scratch[kNaFloats];
 

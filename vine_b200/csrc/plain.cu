@@ -15,6 +15,7 @@
 #include "search.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -53,6 +54,7 @@ __device__ void plain_ctx(Ctx &c, const PlainArgs &A) {
   c.bt.vs = P.vs;
   c.bt.next = P.next;
   c.bt.chain_steps = nullptr;
+  c.bt.spin_limit = P.wait_limit;
   c.bt.epoch = A.st->epoch;
   c.bt.qbase = A.st->qbase;
   c.bt.bcur = A.st->bcur;
@@ -264,6 +266,8 @@ __global__ void plain_finish_kernel(PlainArgs A, int q) {
       s[VINE_STAT_POLICY_CYCLES] = 0;
       s[VINE_STAT_LOAD_CYCLES] = 0;
       s[VINE_STAT_RELAX_CYCLES] = 0;
+      s[VINE_STAT_START_NS] = 0;
+      s[VINE_STAT_TIME_NS] = 0;
     }
   }
 }
@@ -421,6 +425,8 @@ int plain_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *h_src
   P.width0 = r.width0;
   P.len_scale = std::max(1.0f, g->mean_len);
   P.round_cap = r.round_cap;
+  P.wait_limit = c.wait_limit;
+  P.time_limit_ns = 0;  // the host loop below enforces time_limit_ms
   P.table_log2 = c.table_log2;
   P.grid_scope = 1;
   A.st = static_cast<QueryState *>(w.st);
@@ -462,7 +468,21 @@ int plain_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *h_src
     }
     return VINE_OK;
   };
+  std::chrono::steady_clock::time_point t_query;
+  // time_limit_ms on the host clock: checked once per round / bucket
+  auto timed_out = [&]() {
+    if (c.time_limit_ms <= 0) return false;
+    const double ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_query).count();
+    if (ms <= (double)c.time_limit_ms) return false;
+    if (!h.abort) {
+      h.abort = VINE_ERR_TIMEOUT;
+      h.abort_site = kSiteTime;
+    }
+    return true;
+  };
   for (int32_t q = 0; q < nq; ++q) {
+    t_query = std::chrono::steady_clock::now();
     std::memset(&h, 0, sizeof(QueryState));
     h.q = q;
     h.src = h_src[q];
@@ -494,7 +514,7 @@ int plain_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *h_src
         VINE_TRY(push());
         plain_setup_kernel<<<1, 1, 0, stream>>>(args(), q, 1 + which);
         VINE_TRY(pull());
-        while (!h.abort) {
+        while (!h.abort && !timed_out()) {
           const uint32_t avail = h.near_tail - h.near_head;
           if (avail == 0) {
             if (h.far_n == 0) break;
@@ -522,7 +542,7 @@ int plain_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *h_src
       plain_setup_kernel<<<1, 1, 0, stream>>>(args(), q, 3);
       VINE_TRY(pull());
     }
-    while (!h.done && !h.abort) {
+    while (!h.done && !h.abort && !timed_out()) {
       const uint32_t avail = h.near_tail - h.near_head;
       if (avail == 0) {
         // bucket finished: its chains become settled when bcur advances

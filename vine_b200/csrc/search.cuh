@@ -87,6 +87,8 @@ struct SearchParams {
   int sync_rounds; // batch engine: 1 = block-synchronous rounds, 0 = warps pull work
   int binned;      // forward band kept in kBins key bins (batch engine)
   int64_t bin_cap; // labels per bin (far_cap / kBins)
+  long long wait_limit;              // polls / lock attempts of a bounded wait
+  unsigned long long time_limit_ns;  // per query, 0 = none
   const float *mlp;
   float *trace;
   unsigned long long *trace_top;
@@ -97,6 +99,7 @@ struct SearchParams {
 struct __align__(16) QueryState {
   unsigned long long inc_key;  // lexicographic (cost, delay) of the incumbent
   long long t0;
+  unsigned long long g0;  // global timer at the start of the query (ns)
   long long n_expanded, n_relaxed, n_inserted, n_dominated, n_buckets, n_rounds, n_spills;
   unsigned long long n_chain_steps;
   long long n_bound_rounds, bound_cycles;
@@ -206,8 +209,24 @@ __device__ __forceinline__ void fail_query(QueryState &st, int status, int site)
 enum AbortSite {
   kSiteArena = 1, kSiteArenaAlloc = 2, kSiteNear = 3, kSiteBand = 4, kSiteRest = 5,
   kSiteSink = 6, kSiteLock = 7, kSiteRounds = 8, kSitePath = 9, kSiteChunks = 10,
-  kSiteInvalid = 11, kSiteAsync = 12
-};
+  kSiteInvalid = 11, kSiteAsync = 12, kSiteTime = 13, kSiteRing = 14
+};  // the values of enum vine_abort_site (vine.h)
+
+// Device global timer in nanoseconds.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// True (and the query failed with VINE_ERR_TIMEOUT) once the query has run
+// longer than its time limit.
+__device__ __forceinline__ bool over_time(const SearchParams &P, QueryState &st) {
+  if (P.time_limit_ns == 0) return false;
+  if (global_ns() - st.g0 <= P.time_limit_ns) return false;
+  fail_query(st, VINE_ERR_TIMEOUT, kSiteTime);
+  return true;
+}
 
 // Next arena chunk with room for `need` labels: a kept chunk of the worker
 // (reused across its queries) or a new one from the global arena.  Caller has
@@ -263,7 +282,7 @@ __device__ inline void pool_reserve(const SearchParams &P, QueryState &st, uint3
 // when the query failed.
 __device__ inline uint32_t arena_take(const SearchParams &P, QueryState &st, uint32_t need) {
   unsigned long long *pk = reinterpret_cast<unsigned long long *>(&st.chunk_fill);
-  for (int it = 0; it < (1 << 20); ++it) {
+  for (long long it = 0; it < P.wait_limit; ++it) {
     if (*reinterpret_cast<volatile int *>(&st.abort)) return kBadIdx;
     const unsigned long long old = *reinterpret_cast<volatile unsigned long long *>(pk);
     const uint32_t fill = (uint32_t)old, end = (uint32_t)(old >> 32);
@@ -283,7 +302,7 @@ __device__ inline uint32_t arena_take(const SearchParams &P, QueryState &st, uin
       if (!next_chunk(P, st, need, &base, &size)) return;
       atomicExch(pk, ((unsigned long long)(base + size) << 32) | (unsigned long long)(base + need));
       got = base;
-    });
+    }, false, P.wait_limit);
     if (!locked) {
       fail_query(st, VINE_ERR_TIMEOUT, kSiteLock);
       return kBadIdx;
@@ -350,7 +369,7 @@ __device__ __forceinline__ void sink_improve(Ctx &c, int32_t v, float nd, float 
       *ik = key;
       st.inc_idx = idx;
     }
-  }, c.P.grid_scope != 0);
+  }, c.P.grid_scope != 0, c.P.wait_limit);
   if (!ok) fail_query(st, VINE_ERR_TIMEOUT, kSiteLock);
 }
 
@@ -503,10 +522,20 @@ __device__ __forceinline__ void expand_block(Ctx &c, const RoundBuf &rb, uint32_
     for (int b = 0; b < kBatch; ++b) {
       const int i = i0 + b * G;
       idx[b] = i < n ? c.near_ring()[(first + (uint32_t)i) & P.near_mask].x : 0u;
+      if ((uint64_t)idx[b] >= (uint64_t)P.pool_cap) {  // protocol slip: fail, do not follow
+        fail_query(st, VINE_ERR_INTERNAL, kSiteRing);
+        idx[b] = 0u;
+      }
     }
 #pragma unroll
     for (int b = 0; b < kBatch; ++b)
       if (i0 + b * G < n) lab[b] = load_label(&P.pool[idx[b]]);
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (i0 + b * G < n && (uint32_t)(lab[b].vid & 0x7fffffff) >= (uint32_t)P.g.n) {
+        fail_query(st, VINE_ERR_INTERNAL, kSiteRing);
+        lab[b].vid = (int)kDeadBit;  // vertex 0, dead: expands nothing
+      }
 #pragma unroll
     for (int b = 0; b < kBatch; ++b) {
       s[b] = VView{0.0f, true, 0.0f, 0.0f, 0u};
