@@ -2,6 +2,7 @@
 function the headers declare; generators are deterministic and produce the
 advertised shapes; host-side argument checking (no device needed)."""
 import re
+import subprocess
 from pathlib import Path
 
 import numpy as np
@@ -135,3 +136,27 @@ def test_graph_validation_without_device():
     g = v.Graph([0, 1, 1], [1], [-1.0], [1])
     with pytest.raises(v.VineError):
         g.make_gpu_graph()
+
+
+def test_dropin_graph_model_builds_the_csr(tmp_path):
+    """The C++ drop-in's read_graph (COLA format) + adj_to_csr, built and run
+    on the host: the CSR equals the one the file was written from, with edge
+    ids in file order (include/io.hpp:61-91, include/graph.hpp:136-167)."""
+    import cpp_callers as cc
+    from golden_util import load_fixture
+    fx = load_fixture("road_small")
+    gpath = tmp_path / "g.graph"
+    cc.write_cola_graph(gpath, fx["row_ptr"], fx["col"], fx["len"], fx["delay"])
+    exe = cc.build("csr_dump", tmp_path)
+    res = subprocess.run([str(exe), str(gpath), "2"], capture_output=True, text=True, timeout=60)
+    assert res.returncode == 0, res.stderr
+    lines = res.stdout.split("\n")
+    n, m = map(int, lines[0].split())
+    assert (n, m) == (len(fx["row_ptr"]) - 1, len(fx["col"]))
+    row = np.array([int(x) for x in lines[1:n + 2]])
+    assert np.array_equal(row, fx["row_ptr"])
+    slots = np.array([[float(x) for x in ln.split()] for ln in lines[n + 2:n + 2 + m]])
+    assert np.array_equal(slots[:, 0].astype(np.int64), fx["col"])
+    assert np.array_equal(slots[:, 1].astype(np.float32), fx["len"])
+    assert np.array_equal(slots[:, 2].astype(np.float32), fx["delay"])
+    assert np.array_equal(slots[:, 3].astype(np.int64), np.arange(m))  # edge ids in file order
