@@ -209,6 +209,23 @@ int vine_solve_device(vine_graph *g, int32_t nq, const int32_t *src, const int32
                       const float *budget, const vine_config *cfg, vine_results *out,
                       void *stream);
 
+/* Multi-core CPU engine (host arrays only, no device): the reference's
+ * OpenMP solver RUN_CSPP_OMP (algorithm/cspp_cpu.hpp:127-213), behind
+ * cspp::solve_omp / solve_cpu (algorithm/cspp.hpp:55-61), with its data
+ * races removed: each round expands the frontier in parallel, then every
+ * vertex's dominance list is updated by the one thread that owns the vertex.
+ * It is a separate, explicitly chosen solver; the GPU entry points never
+ * fall back to it.  Fills cost / delay / found / status, and when given the
+ * packed paths (path_offsets[nq+1], path, path_capacity) and the sink Pareto
+ * sets (pareto_d / pareto_delay / pareto_n / pareto_stride) of out.
+ * nthreads 0 = all cores; across_queries = 0 runs the queries one after the
+ * other, each expanded by all threads (as the reference does); 1 gives each
+ * thread its own queries.  Same answers either way and for every nthreads. */
+int vine_solve_host(int32_t n, int64_t m, const int64_t *row_ptr, const int32_t *col,
+                    const float *len, const float *delay, int32_t nq, const int32_t *src,
+                    const int32_t *dst, const float *budget, int32_t nthreads,
+                    int32_t across_queries, vine_results *out);
+
 /* ------------------------------------------------------- learned scheduler */
 
 #define VINE_MLP_IN 16

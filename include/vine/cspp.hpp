@@ -346,7 +346,61 @@ class cspp {
     return rc;
   }
 
+  // algorithm/cspp.hpp:55-61: the race-free multi-core CPU engine
+  // (vine_solve_host) on one thread / on all cores; same results as solve().
+  int solve_cpu() { return solve_host(1); }
+  int solve_omp() { return solve_host(0); }
+
   int self_validate() { return 0; }
+
+ private:
+  int solve_host(int nthreads) {
+    if (g->_count_row == nullptr) {
+      if (int rc = g->adj_to_csr()) return rc;
+    }
+    if ((int)init_state.size() < ntask || (int)sink_l.size() < ntask || (int)C_l.size() < ntask)
+      return VINE_ERR_INVALID;
+    const int n = g->N, m = g->_count_row[n];
+    std::vector<int64_t> row((size_t)n + 1);
+    for (int i = 0; i <= n; ++i) row[i] = g->_count_row[i];
+    std::vector<float> len((size_t)m), dly((size_t)m);
+    for (int j = 0; j < m; ++j) {
+      len[j] = g->el ? g->el[g->_eid_col[j]].len : g->_len[j];
+      dly[j] = g->el ? g->el[g->_eid_col[j]].delay : g->_delay[j];
+    }
+    std::vector<int32_t> src(ntask), dst(ntask);
+    std::vector<float> bud(ntask);
+    for (int i = 0; i < ntask; ++i) {
+      src[i] = init_state[i].vid;
+      dst[i] = sink_l[i];
+      bud[i] = C_l[i].delay_L;
+    }
+    cost_l.assign(ntask, 0.0f);
+    delay_l.assign(ntask, 0.0f);
+    found_l.assign(ntask, 0);
+    status_l.assign(ntask, 0);
+    std::vector<int64_t> off((size_t)ntask + 1, 0);
+    std::free(path);
+    const int64_t cap = (int64_t)ntask * (int64_t)(n + 1);  // a path visits each vertex once
+    path = (int *)std::malloc(sizeof(int) * (size_t)std::max<int64_t>(cap, 1));
+    vine_results r = {};
+    r.cost = cost_l.data();
+    r.delay = delay_l.data();
+    r.found = found_l.data();
+    r.status = status_l.data();
+    r.path_offsets = off.data();
+    r.path = path;
+    r.path_capacity = cap;
+    const int rc = vine_solve_host(n, m, row.data(), g->_vid_col, len.data(), dly.data(), ntask,
+                                   src.data(), dst.data(), bud.data(), nthreads, 0, &r);
+    path_l.assign(ntask, nullptr);
+    size_of_result_l.assign(ntask, 0);
+    for (int i = 0; i < ntask; ++i) {
+      path_l[i] = path + off[i];
+      size_of_result_l[i] = (int)(off[i + 1] - off[i]);
+    }
+    return rc;
+  }
 };
 
 #include "io.hpp"

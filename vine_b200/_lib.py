@@ -91,6 +91,9 @@ SIGNATURES = {
                              C.POINTER(vine_config), C.POINTER(vine_results)]),
     "vine_solve_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.POINTER(vine_config), C.POINTER(vine_results), C.c_void_p]),
+    "vine_solve_host": (C.c_int, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_int32, C.c_int32, C.POINTER(vine_results)]),
     "vine_mlp_create": (C.c_int, [C.c_int32, C.c_uint64, C.c_void_p, C.POINTER(C.c_void_p)]),
     "vine_mlp_destroy": (None, [C.c_void_p]),
     "vine_mlp_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -226,6 +226,40 @@ def solve(graph: Graph, src, dst, budget, config=None, paths: bool = True,
     return r
 
 
+def solve_host(graph: Graph, src, dst, budget, nthreads: int = 0, across_queries: bool = False,
+               paths: bool = True, pareto_stride: int = 0, raise_on_error: bool = True) -> Results:
+    """The race-free multi-core CPU engine (vine_solve_host) on the graph's
+    host arrays: an explicitly chosen CPU solver, never a fallback of the GPU
+    entry points."""
+    src = np.ascontiguousarray(src, dtype=np.int32)
+    dst = np.ascontiguousarray(dst, dtype=np.int32)
+    budget = np.ascontiguousarray(budget, dtype=np.float32)
+    nq = int(src.shape[0])
+    r = Results(cost=np.empty(nq, np.float32), delay=np.empty(nq, np.float32),
+                found=np.empty(nq, np.int32), status=np.zeros(nq, np.int32))
+    res = _lib.vine_results()
+    res.cost, res.delay = _ptr(r.cost), _ptr(r.delay)
+    res.found, res.status = _ptr(r.found), _ptr(r.status)
+    cap = max(1024, nq * 4096)
+    if paths:
+        r.path_offsets = np.zeros(nq + 1, np.int64)
+        r.path_vertices = np.zeros(cap, np.int32)
+        res.path_offsets, res.path, res.path_capacity = _ptr(r.path_offsets), _ptr(r.path_vertices), cap
+    if pareto_stride > 0:
+        r.pareto_d = np.zeros((nq, pareto_stride), np.float32)
+        r.pareto_delay = np.zeros((nq, pareto_stride), np.float32)
+        r.pareto_n = np.zeros(nq, np.int32)
+        res.pareto_d, res.pareto_delay = _ptr(r.pareto_d), _ptr(r.pareto_delay)
+        res.pareto_n, res.pareto_stride = _ptr(r.pareto_n), pareto_stride
+    rc = lib.vine_solve_host(graph.N, graph.M, _ptr(graph.row_ptr), _ptr(graph.col),
+                             _ptr(graph.len), _ptr(graph.delay), nq, _ptr(src), _ptr(dst),
+                             _ptr(budget), nthreads, int(across_queries), C.byref(res))
+    r.rc = rc
+    if raise_on_error:
+        check(rc)
+    return r
+
+
 def solve_device(graph: Graph, src, dst, budget, out: dict, config=None, stream=None) -> None:
     """Device-resident solve: src/dst/budget and out[...] are CUDA tensors
     (torch) already in HBM; enqueues on `stream` and returns immediately."""
@@ -281,13 +315,23 @@ class cspp:
         self.size_of_result_l = [len(p) for p in self.path_l]
         return 0
 
+    def _solve_host(self, nthreads: int) -> int:
+        src = np.array([l.vid for l in self.init_state], np.int32)
+        dst = np.array(self.sink_l, np.int32)
+        bud = np.array([c.delay_L for c in self.C_l], np.float32)
+        r = solve_host(self.g, src, dst, bud, nthreads=nthreads)
+        self.cost_l, self.delay_l, self.found_l, self.status_l = r.cost, r.delay, r.found, r.status
+        self.path_l = [r.path(q).copy() for q in range(self.ntask)]
+        self.size_of_result_l = [len(p) for p in self.path_l]
+        return 0
+
     def solve_cpu(self) -> int:
-        raise NotImplementedError(
-            "this engine has no CPU solver; the reference's RUN_CSPP_CPU is only used as the "
-            "test oracle")
+        """algorithm/cspp.hpp:55-57: the host engine on one thread."""
+        return self._solve_host(1)
 
     def solve_omp(self) -> int:
-        return self.solve_cpu()
+        """algorithm/cspp.hpp:59-61: the race-free multi-core host engine."""
+        return self._solve_host(0)
 
 
 # ------------------------------------------------------------------------ MLP
