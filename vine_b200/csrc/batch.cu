@@ -551,6 +551,133 @@ __device__ void reverse_bucket_async(Ctx &c, int which, float radius) {
 // opens (more would spill registers around the inlined insert path).
 constexpr int kSplitBatch = 2;
 
+// ------------------------------------------------- bulk-staged label tiles
+//
+// When a bucket opens, the far bins (and, when the band is rebuilt, the rest
+// pile) are read tile by tile: contiguous runs of 16-byte labels.  Each tile
+// is brought into shared memory by 1-D bulk copies (cp.async.bulk, the TMA
+// engine's untiled form; no multicast: the source is this GPU's own memory)
+// that complete on an mbarrier, double-buffered so the next tile streams in
+// while the block works on the current one.  The labels a tile writes back
+// (compacted in place) land below every position a later tile reads, so the
+// prefetch never races the write-back.
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
+// from global memory to this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Generic-proxy writes of the calling thread become visible to later bulk
+// copies (async proxy) that read the same global / shared memory.
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Two tile buffers and their barriers; `parity` and `busy` are per-thread
+// copies of the same values (every thread waits on every tile).
+struct TileStage {
+  Label *buf[2];
+  uint64_t *bar[2];
+  uint32_t parity;  // bit k: phase parity the next wait on buffer k expects
+  uint32_t busy;    // bit k: a copy into buffer k is in flight
+};
+
+// Waits until buffer k's copies have landed (all threads).  Bounded: after
+// wait_limit polls the query fails with VINE_ERR_TIMEOUT and the worker is
+// marked so that it takes no further query (its buffer may still be written).
+__device__ __forceinline__ bool tile_wait(const SearchParams &P, QueryState &st, TileStage &ts,
+                                          int k) {
+  if (!(ts.busy >> k & 1u)) return true;
+  const uint32_t par = ts.parity >> k & 1u;
+  bool ok = false;
+  for (long long i = 0; i < P.wait_limit; ++i) {
+    if (mbar_try_wait(ts.bar[k], par)) {
+      ok = true;
+      break;
+    }
+    if (i > 8) __nanosleep(64);
+  }
+  ts.busy &= ~(1u << k);
+  ts.parity ^= 1u << k;
+  if (!ok) {
+    fail_query(st, VINE_ERR_TIMEOUT, kSiteTile);
+    st.tile_broken = 1;
+  }
+  return ok;
+}
+
+// Waits for every copy still in flight (before leaving a staged loop early).
+__device__ __forceinline__ void tile_drain(const SearchParams &P, QueryState &st, TileStage &ts) {
+  tile_wait(P, st, ts, 0);
+  tile_wait(P, st, ts, 1);
+}
+
+// Stages labels [base, base + cnt) of a contiguous pile into buffer k
+// (thread 0 issues; every thread records the copy as in flight).
+__device__ __forceinline__ void tile_issue_pile(TileStage &ts, int k, const Label *pile,
+                                                uint32_t base, uint32_t cnt) {
+  if (threadIdx.x == 0) {
+    fence_proxy_async_shared();  // the block's reads of this buffer are done
+    mbar_expect(ts.bar[k], cnt * (uint32_t)sizeof(Label));
+    bulk_load(ts.buf[k], pile + base, cnt * (uint32_t)sizeof(Label), ts.bar[k]);
+  }
+  ts.busy |= 1u << k;
+}
+
+// Stages positions [base, base + cnt) of the scanned bins, seen as one
+// sequence (bin j holds positions [pre[j], pre[j + 1])), into buffer k.
+__device__ __forceinline__ void tile_issue_bins(TileStage &ts, int k, const Label *far,
+                                                int64_t bin_cap, const uint32_t *pre, int last,
+                                                uint32_t base, uint32_t cnt) {
+  if (threadIdx.x == 0) {
+    fence_proxy_async_shared();
+    mbar_expect(ts.bar[k], cnt * (uint32_t)sizeof(Label));
+    const uint32_t end = base + cnt;
+    for (int j = 0; j <= last; ++j) {
+      const uint32_t a = max(base, pre[j]), b = min(end, pre[j + 1]);
+      if (a >= b) continue;
+      bulk_load(ts.buf[k] + (a - base), far + (size_t)j * (size_t)bin_cap + (a - pre[j]),
+                (b - a) * (uint32_t)sizeof(Label), ts.bar[k]);
+    }
+  }
+  ts.busy |= 1u << k;
+}
+
 __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int H = 1 << P.table_log2;
@@ -571,6 +698,14 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   int *scan = r_off + RC;
   QueryState &st = *reinterpret_cast<QueryState *>(
       (reinterpret_cast<uintptr_t>(scan + kScanScratch) + 15) & ~(uintptr_t)15);
+  TileStage ts;
+  ts.buf[0] = reinterpret_cast<Label *>(
+      (reinterpret_cast<uintptr_t>(&st + 1) + 127) & ~(uintptr_t)127);
+  ts.buf[1] = ts.buf[0] + blockDim.x * kSplitBatch;
+  ts.bar[0] = reinterpret_cast<uint64_t *>(ts.buf[1] + blockDim.x * kSplitBatch);
+  ts.bar[1] = ts.bar[0] + 1;
+  ts.parity = 0;
+  ts.busy = 0;
 
   const int tid = threadIdx.x, G = blockDim.x;
   const int slot = blockIdx.x;
@@ -596,6 +731,10 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   for (int i = tid; i < H; i += G) tv[i] = kEmpty;
   for (int i = tid; i < NL; i += G) locks[i] = 0;
   if (tid == 0) {
+    mbar_init(ts.bar[0]);
+    mbar_init(ts.bar[1]);
+    fence_proxy_async_shared();  // the initialised barriers are visible to the copy engine
+    st.tile_broken = 0;
     st.chunk_fill = 0;
     st.chunk_end = 0;
     st.chunk_lock = 0;
@@ -607,8 +746,12 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
 
   for (;;) {
     if (tid == 0) {
-      const unsigned long long k = atomicAdd(P.queue, 1ull);
-      st.q = (k < (unsigned long long)P.nq) ? (P.order ? P.order[k] : (int)k) : -1;
+      if (st.tile_broken) {
+        st.q = -1;  // a tile buffer may still be written: take no further query
+      } else {
+        const unsigned long long k = atomicAdd(P.queue, 1ull);
+        st.q = (k < (unsigned long long)P.nq) ? (P.order ? P.order[k] : (int)k) : -1;
+      }
     }
     __syncthreads();
     const int q = st.q;
@@ -809,21 +952,30 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
           // ---- place, tile by tile; a label whose bin is full stays)
           const uint32_t rn = st.rest_n;
           const uint32_t rtile = (uint32_t)G * kSplitBatch;
-          for (uint32_t base = 0; base < rn; base += rtile) {
+          fence_proxy_async_global();  // this thread's pile writes, before the bulk reads
+          __syncthreads();
+          if (rn > 0) tile_issue_pile(ts, 0, c.rest, 0, min(rtile, rn));
+          for (uint32_t base = 0, t = 0; base < rn; base += rtile, ++t) {
+            const int k = (int)(t & 1u);
             if (tid == 0) pool_reserve(P, st, rtile);  // for labels offered directly
+            if (base + rtile < rn)  // the other buffer was released by the last barrier
+              tile_issue_pile(ts, k ^ 1, c.rest, base + rtile, min(rtile, rn - base - rtile));
             __syncthreads();
-            if (st.abort) break;
+            const bool landed = tile_wait(P, st, ts, k);
+            if (__syncthreads_or(!landed || st.abort)) {  // the same decision in every thread
+              tile_drain(P, st, ts);
+              break;
+            }
             Label item[kSplitBatch];
             float f[kSplitBatch];
 #pragma unroll
             for (int b = 0; b < kSplitBatch; ++b) {
               const uint32_t i = base + (uint32_t)(b * G + tid);
-              if (i < rn) item[b] = c.rest[i];
+              if (i < rn) item[b] = ts.buf[k][b * G + tid];
             }
 #pragma unroll
             for (int b = 0; b < kSplitBatch; ++b)
               if (base + (uint32_t)(b * G + tid) < rn) f[b] = key_of(c, item[b].vid, item[b].d);
-            __syncthreads();  // the whole tile is read before it is overwritten
 #pragma unroll
             for (int b = 0; b < kSplitBatch; ++b) {
               if (base + (uint32_t)(b * G + tid) >= rn) break;
@@ -870,10 +1022,21 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
         const int last = st.bin_last;
         const uint32_t fn = st.bin_pre[last + 1];
         const uint32_t tile = (uint32_t)G * kSplitBatch;
-        for (uint32_t base = 0; base < fn; base += tile) {
+        fence_proxy_async_global();  // this thread's bin writes, before the bulk reads
+        __syncthreads();
+        if (fn > 0) tile_issue_bins(ts, 0, c.far, P.bin_cap, st.bin_pre, last, 0, min(tile, fn));
+        for (uint32_t base = 0, t = 0; base < fn; base += tile, ++t) {
+          const int k = (int)(t & 1u);
           if (tid == 0) pool_reserve(P, st, tile);
+          if (base + tile < fn)  // the other buffer was released by the last barrier
+            tile_issue_bins(ts, k ^ 1, c.far, P.bin_cap, st.bin_pre, last, base + tile,
+                            min(tile, fn - base - tile));
           __syncthreads();
-          if (st.abort) break;
+          const bool landed = tile_wait(P, st, ts, k);
+          if (__syncthreads_or(!landed || st.abort)) {  // the same decision in every thread
+            tile_drain(P, st, ts);
+            break;
+          }
           Label item[kSplitBatch];
           VView sv[kSplitBatch];
           int bj[kSplitBatch];
@@ -885,13 +1048,12 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
               int j = 0;
               while (j < last && st.bin_pre[j + 1] <= i) ++j;
               bj[b] = j;
-              item[b] = c.far[(size_t)j * (size_t)P.bin_cap + (i - st.bin_pre[j])];
+              item[b] = ts.buf[k][b * G + tid];
             }
           }
 #pragma unroll
           for (int b = 0; b < kSplitBatch; ++b)
             if (base + (uint32_t)(b * G + tid) < fn) sv[b] = c.view(item[b].vid);
-          __syncthreads();  // the whole tile is read before it is overwritten
 #pragma unroll
           for (int b = 0; b < kSplitBatch; ++b) {
             if (base + (uint32_t)(b * G + tid) >= fn) break;
@@ -1036,12 +1198,14 @@ __global__ void epoch_kernel(unsigned long long *counters, int32_t nq) {
   counters[4] += (unsigned long long)nq;
 }
 
-size_t batch_smem_bytes(int table_log2, int lock_log2, int round_cap) {
+size_t batch_smem_bytes(int table_log2, int lock_log2, int round_cap, int block_threads) {
   size_t b = ((sizeof(int32_t) + sizeof(float2) + sizeof(uint32_t)) << table_log2) +
              (sizeof(int) << lock_log2) +
              (size_t)round_cap * 24 + kScanScratch * sizeof(int);
   b = (b + 15) & ~(size_t)15;
-  return b + sizeof(QueryState) + 16;
+  b += sizeof(QueryState) + 16;
+  // two staged label tiles (128-byte aligned) and their barriers
+  return b + 128 + 2 * (size_t)block_threads * kSplitBatch * sizeof(Label) + 2 * sizeof(uint64_t);
 }
 
 int lock_log2_for(int table_log2) { return std::max(5, table_log2 - 1); }
@@ -1146,7 +1310,7 @@ int batch_prepare(vine_graph *g, const Resolved &r, int32_t nq, cudaStream_t str
   }
   w.epoch_next += (uint32_t)nq;
   const size_t smem = batch_smem_bytes(r.cfg.table_log2, lock_log2_for(r.cfg.table_log2),
-                                       r.cfg.sync_rounds ? r.round_cap : 0);
+                                       r.cfg.sync_rounds ? r.round_cap : 0, r.cfg.block_threads);
   VINE_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
   return VINE_OK;
@@ -1222,7 +1386,8 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.trace_top = w.counters + 3;
   P.trace_cap = w.trace_cap;
 
-  const size_t smem = batch_smem_bytes(c.table_log2, P.lock_log2, c.sync_rounds ? r.round_cap : 0);
+  const size_t smem =
+      batch_smem_bytes(c.table_log2, P.lock_log2, c.sync_rounds ? r.round_cap : 0, c.block_threads);
   VINE_CUDA_TRY(cudaMemsetAsync(w.counters, 0, sizeof(unsigned long long) * 4, stream));
   epoch_kernel<<<1, 1, 0, stream>>>(w.counters, nq);
   if (c.order_queries) VINE_TRY(order_queries(nq, d_budget, w.order, stream));
@@ -1245,7 +1410,8 @@ int batch_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d_src
 
 int batch_slots(const vine_graph *g, const vine_config &c, int round_cap, int *slots) {
   const size_t smem =
-      batch_smem_bytes(c.table_log2, lock_log2_for(c.table_log2), c.sync_rounds ? round_cap : 0);
+      batch_smem_bytes(c.table_log2, lock_log2_for(c.table_log2), c.sync_rounds ? round_cap : 0,
+                       c.block_threads);
   VINE_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
   int per_sm = 0;

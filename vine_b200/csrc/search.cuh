@@ -136,6 +136,7 @@ struct __align__(16) QueryState {
 
   int abort;
   int done;
+  int tile_broken;  // a staged tile's copy never landed: the worker stops
   int split_cap;
   int hist_n;
   uint32_t sink_n;
@@ -209,7 +210,7 @@ __device__ __forceinline__ void fail_query(QueryState &st, int status, int site)
 enum AbortSite {
   kSiteArena = 1, kSiteArenaAlloc = 2, kSiteNear = 3, kSiteBand = 4, kSiteRest = 5,
   kSiteSink = 6, kSiteLock = 7, kSiteRounds = 8, kSitePath = 9, kSiteChunks = 10,
-  kSiteInvalid = 11, kSiteAsync = 12, kSiteTime = 13, kSiteRing = 14
+  kSiteInvalid = 11, kSiteAsync = 12, kSiteTime = 13, kSiteRing = 14, kSiteTile = 15
 };  // the values of enum vine_abort_site (vine.h)
 
 // Device global timer in nanoseconds.
