@@ -211,6 +211,39 @@ int vine_solve_device(vine_graph *g, int32_t nq, const int32_t *src, const int32
                       const float *budget, const vine_config *cfg, vine_results *out,
                       void *stream);
 
+/* ---------------------------------------------------------- label variants */
+
+/* The reference's other label types (include/label.hpp:46-465 with
+ * include/constraint.hpp:21-187), chosen there at compile time by the CSP
+ * macro, here per call. */
+enum vine_label_kind {
+  VINE_LABEL_CSP = 1,     /* (d, delay): delay <= L (CSP=1; CSP=4 is the same) */
+  VINE_LABEL_HOP = 2,     /* (d, delay, hop): delay <= L and hop <= H (CSP=2)  */
+  VINE_LABEL_MAXCOST = 3, /* (d, delay, hop, maxcost = largest arc length):
+                             delay <= L, hop <= H, maxcost <= M (CSP=3)        */
+  VINE_LABEL_QOS = 6      /* (d, bandwidth = smallest arc delay on the path,
+                             21474836 at the source): bandwidth >= L          */
+};
+
+/* Solves nq queries of label kind `kind` on the GPU (host buffers) with the
+ * variant engine: every label is checked against all stored labels of its
+ * vertex under the kind's dominance, so any number of criteria is exact.
+ * delay_limit[q] is L (the bandwidth floor for QoS); hop_limit[q] (H,
+ * default 100 when NULL) and maxcost_limit[q] (M, default 10000 when NULL)
+ * as in the reference's constraints.  The answer is the best feasible sink
+ * label: lexicographically smallest (d, delay, hop, maxcost); for QoS the
+ * smallest d, then the largest bandwidth.  out->cost / delay receive its d
+ * and delay (QoS: bandwidth); extra[2q], extra[2q+1] (may be NULL) its hop
+ * count and maxcost.  Paths as in vine_solve; Pareto outputs are not
+ * filled.  cfg: bucket_width, block_threads (default 256), max_workers,
+ * pool_labels, far_capacity, wait_limit, time_limit_ms are used.
+ * Replaces cspp<c_label,c_edge>::solve for a reference built with CSP=2, 3
+ * or the QoS label (algorithm/cspp.hpp:48-53). */
+int vine_solve_labels(vine_graph *g, int32_t kind, int32_t nq, const int32_t *src,
+                      const int32_t *dst, const float *delay_limit, const float *hop_limit,
+                      const float *maxcost_limit, const vine_config *cfg, vine_results *out,
+                      float *extra);
+
 /* Multi-core CPU engine (host arrays only, no device): the reference's
  * OpenMP solver RUN_CSPP_OMP (algorithm/cspp_cpu.hpp:127-213), behind
  * cspp::solve_omp / solve_cpu (algorithm/cspp.hpp:55-61), with its data

@@ -91,6 +91,8 @@ def _lib_ref():
         lib.ref_solve_capped.argtypes = [vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_double, vp,
                                          vp, vp, vp, vp]
         lib.ref_last_error.restype = C.c_char_p
+        lib.ref_solve_variant.argtypes = [vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_int32,
+                                          C.c_double, vp, vp, vp, vp, C.c_int32, vp, vp]
         lib.vine_workload_default_params.argtypes = [C.c_int32, vp]
         lib.vine_workload_generate.argtypes = [vp, C.POINTER(vp)]
         lib.vine_workload_graph.argtypes = [vp] + [vp] * 6
@@ -241,6 +243,36 @@ class RefSolver:
             raise RuntimeError("ref_solve_capped failed")
         return {"seconds": secs, "finished": fin.astype(bool), "cost": cost, "delay": delay,
                 "found": found.astype(bool)}
+
+    def solve_variant(self, kind: int, src, dst, delay_L, hop_L=None, max_L=None,
+                      nthreads: int = 1, cap_seconds: float = 0.0, record_paths: bool = False):
+        """A label variant through the reference's RUN_CSPP_CPU: kind 2
+        hop-constrained, 3 max-cost, 6 QoS bottleneck.  Returns best[q] =
+        (d, delay, hop, maxcost) (QoS: (d, bandwidth, 0, 0)), found,
+        finished (False when stopped at cap_seconds), paths."""
+        src = np.ascontiguousarray(src, np.int32)
+        dst = np.ascontiguousarray(dst, np.int32)
+        nq = src.shape[0]
+        dL = np.ascontiguousarray(delay_L, np.float32)
+        hL = np.ascontiguousarray(hop_L if hop_L is not None else np.full(nq, 100), np.int32)
+        mL = np.ascontiguousarray(max_L if max_L is not None else np.full(nq, 10000), np.float32)
+        best = np.zeros((nq, 4), np.float32)
+        found = np.zeros(nq, np.int32)
+        fin = np.zeros(nq, np.int32)
+        stride = self.g.n + 1 if record_paths else 0
+        paths = np.zeros((nq, stride), np.int32) if record_paths else None
+        plen = np.zeros(nq, np.int32) if record_paths else None
+        calls = np.zeros(nq, np.int64)
+        rc = self.lib.ref_solve_variant(self.h, kind, nq, _p(src), _p(dst), _p(dL), _p(hL), _p(mL),
+                                        nthreads, float(cap_seconds), _p(best), _p(found), _p(fin),
+                                        _p(paths), stride, _p(plen), _p(calls))
+        if rc != 0:
+            raise ValueError("ref_solve_variant failed")
+        out = {"best": best, "found": found.astype(bool), "finished": fin.astype(bool),
+               "calls": calls}
+        if record_paths:
+            out["paths"] = [paths[q, : plen[q]].copy() for q in range(nq)]
+        return out
 
     def close(self):
         if self.h:

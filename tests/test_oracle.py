@@ -117,3 +117,37 @@ def test_host_generator_copy_matches_library(oracle_mod, cid, over):
     b = v.Workload.generate(cid, **over)
     for k in ("row_ptr", "col", "len", "delay", "src", "dst", "budget", "alpha"):
         assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_variant_golden_reproduces_and_hand_answers(oracle_mod):
+    """tests/golden/variants.json is what the reference's solver (built with
+    the variant labels) returns, and its 3-vertex cases are the hand-checked
+    answers: hop limit 1 forces the direct arc (20), the QoS floor 3 leaves
+    only the direct arc (bandwidth 1 < 3 fails, so no path) ..."""
+    import json
+    O = oracle_mod
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    from golden_util import GOLDEN
+    var = json.loads((GOLDEN / "variants.json").read_text())
+    for name in ("kat3", "road_small"):
+        fx = load_fixture(name)
+        g = O.CsrGraph(fx["row_ptr"], fx["col"], fx["len"], fx["delay"])
+        ref = O.RefSolver(g)
+        for kind, k in (("hop", 2), ("maxcost", 3), ("qos", 6)):
+            qs = var[name][kind]
+            r = ref.solve_variant(k, [e["src"] for e in qs], [e["dst"] for e in qs],
+                                  [e["delay_L"] for e in qs], [e.get("hop_L", 100) for e in qs],
+                                  [e.get("max_L", 10000.0) for e in qs], nthreads=4)
+            for q, e in enumerate(qs):
+                assert bool(r["found"][q]) == e["found"]
+                if e["found"]:
+                    assert [float(x) for x in r["best"][q]] == e["best"]
+        ref.close()
+    r = O.RefSolver(O.CsrGraph(*[load_fixture("kat3")[k] for k in ("row_ptr", "col", "len", "delay")]))
+    hop = r.solve_variant(2, [0, 0], [2, 2], [100, 100], [2, 1])
+    assert hop["best"][0][:3].tolist() == [12, 5, 2] and hop["best"][1][:3].tolist() == [20, 1, 1]
+    qos = r.solve_variant(6, [0, 0], [2, 2], [2, 3])
+    # 0-1-2 has bandwidth min(2, 3) = 2; the direct arc has bandwidth 1
+    assert qos["best"][0][:2].tolist() == [12, 2] and not qos["found"][1]
+    r.close()

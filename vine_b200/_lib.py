@@ -30,6 +30,7 @@ STATUS_NAMES = {
 }
 
 ENGINE_BATCH, ENGINE_PLAIN = 0, 1
+LABEL_CSP, LABEL_HOP, LABEL_MAXCOST, LABEL_QOS = 1, 2, 3, 6
 MODE_OPTIMAL, MODE_PARETO = 0, 1
 POLICY_FIXED, POLICY_AR, POLICY_MLP = 0, 1, 2
 STAT_NAMES = ["expanded", "relaxed", "inserted", "dominated", "buckets", "rounds", "spills",
@@ -91,6 +92,9 @@ SIGNATURES = {
                              C.POINTER(vine_config), C.POINTER(vine_results)]),
     "vine_solve_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.POINTER(vine_config), C.POINTER(vine_results), C.c_void_p]),
+    "vine_solve_labels": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(vine_config),
+                                    C.POINTER(vine_results), C.c_void_p]),
     "vine_solve_host": (C.c_int, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_int32, C.c_int32, C.POINTER(vine_results)]),

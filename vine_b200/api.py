@@ -171,6 +171,7 @@ class Results:
     stats: Optional[np.ndarray] = None
     rc: int = 0
     retried: int = 0
+    extra: Optional[np.ndarray] = None  # label variants: [nq, 2] hop count, maxcost
 
     def path(self, q: int) -> np.ndarray:
         a, b = self.path_offsets[q], self.path_offsets[q + 1]
@@ -221,6 +222,47 @@ def solve(graph: Graph, src, dst, budget, config=None, paths: bool = True,
                      path_capacity=int(r.path_offsets[nq]), raise_on_error=raise_on_error)
     r.rc = rc
     r.retried = int(res.retried)
+    if raise_on_error:
+        check(rc)
+    return r
+
+
+LABEL_KINDS = {"csp": _lib.LABEL_CSP, "hop": _lib.LABEL_HOP, "maxcost": _lib.LABEL_MAXCOST,
+               "qos": _lib.LABEL_QOS}
+
+
+def solve_labels(graph: Graph, kind, src, dst, delay_limit, hop_limit=None, maxcost_limit=None,
+                 config=None, paths: bool = True, stats: bool = False,
+                 raise_on_error: bool = True) -> Results:
+    """Label-variant queries on the GPU (vine_solve_labels): kind "csp",
+    "hop", "maxcost" or "qos" (the reference's CSP=1/4, 2, 3 and QoS labels).
+    Results carry cost (d), delay (QoS: bandwidth) and `extra` [nq, 2] (hop
+    count, maxcost) of the best feasible sink label."""
+    k = LABEL_KINDS[kind] if isinstance(kind, str) else int(kind)
+    src = np.ascontiguousarray(src, dtype=np.int32)
+    dst = np.ascontiguousarray(dst, dtype=np.int32)
+    nq = int(src.shape[0])
+    dL = np.ascontiguousarray(delay_limit, dtype=np.float32)
+    hL = None if hop_limit is None else np.ascontiguousarray(hop_limit, dtype=np.float32)
+    mL = None if maxcost_limit is None else np.ascontiguousarray(maxcost_limit, dtype=np.float32)
+    r = Results(cost=np.empty(nq, np.float32), delay=np.empty(nq, np.float32),
+                found=np.empty(nq, np.int32), status=np.zeros(nq, np.int32))
+    r.extra = np.zeros((nq, 2), np.float32)
+    res = _lib.vine_results()
+    res.cost, res.delay = _ptr(r.cost), _ptr(r.delay)
+    res.found, res.status = _ptr(r.found), _ptr(r.status)
+    if paths:
+        cap = max(1024, nq * 4096)
+        r.path_offsets = np.zeros(nq + 1, np.int64)
+        r.path_vertices = np.zeros(cap, np.int32)
+        res.path_offsets, res.path, res.path_capacity = _ptr(r.path_offsets), _ptr(r.path_vertices), cap
+    if stats:
+        r.stats = np.zeros((nq, _lib.STAT_COUNT), np.int64)
+        res.stats = _ptr(r.stats)
+    cfg = config if config is not None else Config()
+    rc = lib.vine_solve_labels(graph.handle, k, nq, _ptr(src), _ptr(dst), _ptr(dL), _ptr(hL),
+                               _ptr(mL), C.byref(cfg), C.byref(res), _ptr(r.extra))
+    r.rc = rc
     if raise_on_error:
         check(rc)
     return r
