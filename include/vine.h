@@ -118,7 +118,11 @@ typedef struct {
                               a query still running after it stops with
                               VINE_ERR_TIMEOUT (0 = 600000, i.e. 10 minutes;
                               < 0 = no limit)                                 */
-  int32_t reserved[1];
+  int32_t split_staging;   /* batch engine: 1 = when a bucket opens, stream its
+                              far-bin / rest-pile label tiles into shared
+                              memory with bulk copies (cp.async.bulk) instead
+                              of per-thread loads; costs 64 bytes of shared
+                              memory (taken from L1) per thread            */
 } vine_config;
 
 void vine_config_default(vine_config *cfg);

@@ -41,6 +41,7 @@ CASES = [pytest.param(n, id=_case_id(n)) for n in SCALE_CASES]
 CONFIGS = {
     "bench": dict(engine="batch", policy="ar", use_bounds=1, bucket_width_mult=0.3),
     "nobounds": dict(engine="batch", policy="fixed", use_bounds=0),
+    "staged": dict(engine="batch", policy="ar", use_bounds=1, split_staging=1, bucket_width_mult=0.3),
 }
 
 
@@ -58,6 +59,8 @@ def test_full_size_matches_expected(name, cfg):
     import vine_b200 as v
     if not scale_fixture_path(name).exists():
         pytest.fail(f"fixture scale_{name}.json missing")
+    if cfg == "staged" and name not in ("c4_chunglu100k", "c5_sample256"):
+        pytest.skip("staged tiles are checked at full size on the hub graph and the bench sample")
     if cfg == "nobounds" and name in ("c3_road1500k", "c2_road264k"):
         # without bounds a 1.5M-vertex random-pair query explores most of the
         # graph; the bounded configuration covers these two at full size

@@ -54,7 +54,7 @@ class vine_config(C.Structure):
         ("split_threshold", C.c_int32), ("pool_labels", C.c_int64), ("far_capacity", C.c_int64),
         ("use_cuda_graph", C.c_int32), ("order_queries", C.c_int32), ("mlp", C.c_void_p),
         ("trace", C.c_int32), ("max_workers", C.c_int32), ("sync_rounds", C.c_int32), ("band_mult", C.c_int32), ("ar_scale", C.c_float),
-        ("wait_limit", C.c_int32), ("time_limit_ms", C.c_int32), ("reserved", C.c_int32 * 1),
+        ("wait_limit", C.c_int32), ("time_limit_ms", C.c_int32), ("split_staging", C.c_int32),
     ]
 
 

@@ -151,7 +151,7 @@ def Config(**kw) -> _lib.vine_config:
 
 
 def config_dict(c: _lib.vine_config) -> dict:
-    return {k: getattr(c, k) for k, _ in _lib.vine_config._fields_ if k not in ("mlp", "reserved")}
+    return {k: getattr(c, k) for k, _ in _lib.vine_config._fields_ if k != "mlp"}
 
 
 # --------------------------------------------------------------------- results

@@ -730,10 +730,13 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
 
   for (int i = tid; i < H; i += G) tv[i] = kEmpty;
   for (int i = tid; i < NL; i += G) locks[i] = 0;
+  const bool stage = P.split_staging != 0;
   if (tid == 0) {
-    mbar_init(ts.bar[0]);
-    mbar_init(ts.bar[1]);
-    fence_proxy_async_shared();  // the initialised barriers are visible to the copy engine
+    if (stage) {
+      mbar_init(ts.bar[0]);
+      mbar_init(ts.bar[1]);
+      fence_proxy_async_shared();  // the initialised barriers are visible to the copy engine
+    }
     st.tile_broken = 0;
     st.chunk_fill = 0;
     st.chunk_end = 0;
@@ -952,18 +955,20 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
           // ---- place, tile by tile; a label whose bin is full stays)
           const uint32_t rn = st.rest_n;
           const uint32_t rtile = (uint32_t)G * kSplitBatch;
-          fence_proxy_async_global();  // this thread's pile writes, before the bulk reads
-          __syncthreads();
-          if (rn > 0) tile_issue_pile(ts, 0, c.rest, 0, min(rtile, rn));
+          if (stage) {
+            fence_proxy_async_global();  // this thread's pile writes, before the bulk reads
+            __syncthreads();
+            if (rn > 0) tile_issue_pile(ts, 0, c.rest, 0, min(rtile, rn));
+          }
           for (uint32_t base = 0, t = 0; base < rn; base += rtile, ++t) {
             const int k = (int)(t & 1u);
             if (tid == 0) pool_reserve(P, st, rtile);  // for labels offered directly
-            if (base + rtile < rn)  // the other buffer was released by the last barrier
+            if (stage && base + rtile < rn)  // the other buffer was released by the last barrier
               tile_issue_pile(ts, k ^ 1, c.rest, base + rtile, min(rtile, rn - base - rtile));
             __syncthreads();
-            const bool landed = tile_wait(P, st, ts, k);
+            const bool landed = stage ? tile_wait(P, st, ts, k) : true;
             if (__syncthreads_or(!landed || st.abort)) {  // the same decision in every thread
-              tile_drain(P, st, ts);
+              if (stage) tile_drain(P, st, ts);
               break;
             }
             Label item[kSplitBatch];
@@ -971,11 +976,12 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
 #pragma unroll
             for (int b = 0; b < kSplitBatch; ++b) {
               const uint32_t i = base + (uint32_t)(b * G + tid);
-              if (i < rn) item[b] = ts.buf[k][b * G + tid];
+              if (i < rn) item[b] = stage ? ts.buf[k][b * G + tid] : c.rest[i];
             }
 #pragma unroll
             for (int b = 0; b < kSplitBatch; ++b)
               if (base + (uint32_t)(b * G + tid) < rn) f[b] = key_of(c, item[b].vid, item[b].d);
+            if (!stage) __syncthreads();  // the whole tile is read before it is overwritten
 #pragma unroll
             for (int b = 0; b < kSplitBatch; ++b) {
               if (base + (uint32_t)(b * G + tid) >= rn) break;
@@ -1022,19 +1028,21 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
         const int last = st.bin_last;
         const uint32_t fn = st.bin_pre[last + 1];
         const uint32_t tile = (uint32_t)G * kSplitBatch;
-        fence_proxy_async_global();  // this thread's bin writes, before the bulk reads
-        __syncthreads();
-        if (fn > 0) tile_issue_bins(ts, 0, c.far, P.bin_cap, st.bin_pre, last, 0, min(tile, fn));
+        if (stage) {
+          fence_proxy_async_global();  // this thread's bin writes, before the bulk reads
+          __syncthreads();
+          if (fn > 0) tile_issue_bins(ts, 0, c.far, P.bin_cap, st.bin_pre, last, 0, min(tile, fn));
+        }
         for (uint32_t base = 0, t = 0; base < fn; base += tile, ++t) {
           const int k = (int)(t & 1u);
           if (tid == 0) pool_reserve(P, st, tile);
-          if (base + tile < fn)  // the other buffer was released by the last barrier
+          if (stage && base + tile < fn)  // the other buffer was released by the last barrier
             tile_issue_bins(ts, k ^ 1, c.far, P.bin_cap, st.bin_pre, last, base + tile,
                             min(tile, fn - base - tile));
           __syncthreads();
-          const bool landed = tile_wait(P, st, ts, k);
+          const bool landed = stage ? tile_wait(P, st, ts, k) : true;
           if (__syncthreads_or(!landed || st.abort)) {  // the same decision in every thread
-            tile_drain(P, st, ts);
+            if (stage) tile_drain(P, st, ts);
             break;
           }
           Label item[kSplitBatch];
@@ -1048,12 +1056,14 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
               int j = 0;
               while (j < last && st.bin_pre[j + 1] <= i) ++j;
               bj[b] = j;
-              item[b] = ts.buf[k][b * G + tid];
+              item[b] = stage ? ts.buf[k][b * G + tid]
+                              : c.far[(size_t)j * (size_t)P.bin_cap + (i - st.bin_pre[j])];
             }
           }
 #pragma unroll
           for (int b = 0; b < kSplitBatch; ++b)
             if (base + (uint32_t)(b * G + tid) < fn) sv[b] = c.view(item[b].vid);
+          if (!stage) __syncthreads();  // the whole tile is read before it is overwritten
 #pragma unroll
           for (int b = 0; b < kSplitBatch; ++b) {
             if (base + (uint32_t)(b * G + tid) >= fn) break;
@@ -1198,12 +1208,14 @@ __global__ void epoch_kernel(unsigned long long *counters, int32_t nq) {
   counters[4] += (unsigned long long)nq;
 }
 
-size_t batch_smem_bytes(int table_log2, int lock_log2, int round_cap, int block_threads) {
+size_t batch_smem_bytes(int table_log2, int lock_log2, int round_cap, int block_threads,
+                        int staging) {
   size_t b = ((sizeof(int32_t) + sizeof(float2) + sizeof(uint32_t)) << table_log2) +
              (sizeof(int) << lock_log2) +
              (size_t)round_cap * 24 + kScanScratch * sizeof(int);
   b = (b + 15) & ~(size_t)15;
   b += sizeof(QueryState) + 16;
+  if (!staging) return b;
   // two staged label tiles (128-byte aligned) and their barriers
   return b + 128 + 2 * (size_t)block_threads * kSplitBatch * sizeof(Label) + 2 * sizeof(uint64_t);
 }
@@ -1310,7 +1322,8 @@ int batch_prepare(vine_graph *g, const Resolved &r, int32_t nq, cudaStream_t str
   }
   w.epoch_next += (uint32_t)nq;
   const size_t smem = batch_smem_bytes(r.cfg.table_log2, lock_log2_for(r.cfg.table_log2),
-                                       r.cfg.sync_rounds ? r.round_cap : 0, r.cfg.block_threads);
+                                       r.cfg.sync_rounds ? r.round_cap : 0, r.cfg.block_threads,
+                                       r.cfg.split_staging);
   VINE_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
   return VINE_OK;
@@ -1379,6 +1392,7 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.lock_log2 = lock_log2_for(c.table_log2);
   P.probe = 16;
   P.grid_scope = 0;
+  P.split_staging = c.split_staging;
   P.wait_limit = c.wait_limit;
   P.time_limit_ns = c.time_limit_ms > 0 ? (unsigned long long)c.time_limit_ms * 1000000ull : 0ull;
   P.mlp = (c.policy == VINE_POLICY_MLP && c.mlp) ? c.mlp->params : nullptr;
@@ -1386,8 +1400,8 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.trace_top = w.counters + 3;
   P.trace_cap = w.trace_cap;
 
-  const size_t smem =
-      batch_smem_bytes(c.table_log2, P.lock_log2, c.sync_rounds ? r.round_cap : 0, c.block_threads);
+  const size_t smem = batch_smem_bytes(c.table_log2, P.lock_log2, c.sync_rounds ? r.round_cap : 0,
+                                       c.block_threads, c.split_staging);
   VINE_CUDA_TRY(cudaMemsetAsync(w.counters, 0, sizeof(unsigned long long) * 4, stream));
   epoch_kernel<<<1, 1, 0, stream>>>(w.counters, nq);
   if (c.order_queries) VINE_TRY(order_queries(nq, d_budget, w.order, stream));
@@ -1411,7 +1425,7 @@ int batch_run(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d_src
 int batch_slots(const vine_graph *g, const vine_config &c, int round_cap, int *slots) {
   const size_t smem =
       batch_smem_bytes(c.table_log2, lock_log2_for(c.table_log2), c.sync_rounds ? round_cap : 0,
-                       c.block_threads);
+                       c.block_threads, c.split_staging);
   VINE_CUDA_TRY(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
   int per_sm = 0;

@@ -87,6 +87,7 @@ struct SearchParams {
   int sync_rounds; // batch engine: 1 = block-synchronous rounds, 0 = warps pull work
   int binned;      // forward band kept in kBins key bins (batch engine)
   int64_t bin_cap; // labels per bin (far_cap / kBins)
+  int split_staging;                 // bucket opening reads tiles through bulk copies
   long long wait_limit;              // polls / lock attempts of a bounded wait
   unsigned long long time_limit_ns;  // per query, 0 = none
   const float *mlp;
