@@ -215,6 +215,19 @@ int vine_solve_device(vine_graph *g, int32_t nq, const int32_t *src, const int32
                       const float *budget, const vine_config *cfg, vine_results *out,
                       void *stream);
 
+/* Splits one batch over several GPUs: graphs[k] is the same graph created on
+ * device k (vine_graph_create per device).  Queries are independent, so
+ * there is no exchange between devices: each solves its share with
+ * vine_solve on its own host thread, and results land in `out` in query
+ * order (paths packed as in vine_solve; out->retried sums the shares).
+ * Shares are chosen longest-first by budget, so every device gets a similar
+ * mix of heavy and light queries.  The reference runs one device
+ * (main.cu:50); this is the query-replica scaling of its query loop
+ * (algorithm/cspp.cuh:134-296). */
+int vine_solve_multi(vine_graph **graphs, int32_t ngraphs, int32_t nq, const int32_t *src,
+                     const int32_t *dst, const float *budget, const vine_config *cfg,
+                     vine_results *out);
+
 /* ---------------------------------------------------------- label variants */
 
 /* The reference's other label types (include/label.hpp:46-465 with

@@ -92,6 +92,8 @@ SIGNATURES = {
                              C.POINTER(vine_config), C.POINTER(vine_results)]),
     "vine_solve_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.POINTER(vine_config), C.POINTER(vine_results), C.c_void_p]),
+    "vine_solve_multi": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.POINTER(vine_config), C.POINTER(vine_results)]),
     "vine_solve_labels": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(vine_config),
                                     C.POINTER(vine_results), C.c_void_p]),

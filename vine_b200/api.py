@@ -227,6 +227,38 @@ def solve(graph: Graph, src, dst, budget, config=None, paths: bool = True,
     return r
 
 
+def solve_multi(graphs: Sequence[Graph], src, dst, budget, config=None, paths: bool = True,
+                stats: bool = False, raise_on_error: bool = True) -> Results:
+    """One batch split over several graph handles (one per device) by
+    vine_solve_multi; results in query order."""
+    src = np.ascontiguousarray(src, dtype=np.int32)
+    dst = np.ascontiguousarray(dst, dtype=np.int32)
+    budget = np.ascontiguousarray(budget, dtype=np.float32)
+    nq = int(src.shape[0])
+    r = Results(cost=np.empty(nq, np.float32), delay=np.empty(nq, np.float32),
+                found=np.empty(nq, np.int32), status=np.zeros(nq, np.int32))
+    res = _lib.vine_results()
+    res.cost, res.delay = _ptr(r.cost), _ptr(r.delay)
+    res.found, res.status = _ptr(r.found), _ptr(r.status)
+    if paths:
+        cap = max(1024, nq * 4096)
+        r.path_offsets = np.zeros(nq + 1, np.int64)
+        r.path_vertices = np.zeros(cap, np.int32)
+        res.path_offsets, res.path, res.path_capacity = _ptr(r.path_offsets), _ptr(r.path_vertices), cap
+    if stats:
+        r.stats = np.zeros((nq, _lib.STAT_COUNT), np.int64)
+        res.stats = _ptr(r.stats)
+    handles = (C.c_void_p * len(graphs))(*[gr.handle.value for gr in graphs])
+    cfg = config if config is not None else Config()
+    rc = lib.vine_solve_multi(handles, len(graphs), nq, _ptr(src), _ptr(dst), _ptr(budget),
+                              C.byref(cfg), C.byref(res))
+    r.rc = rc
+    r.retried = int(res.retried)
+    if raise_on_error:
+        check(rc)
+    return r
+
+
 LABEL_KINDS = {"csp": _lib.LABEL_CSP, "hop": _lib.LABEL_HOP, "maxcost": _lib.LABEL_MAXCOST,
                "qos": _lib.LABEL_QOS}
 
