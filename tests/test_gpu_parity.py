@@ -21,11 +21,11 @@ CONFIGS = {
     "batch_bounds_narrow": dict(engine="batch", use_bounds=1, bucket_width=5.0, block_threads=256),
     "batch_sync_rounds": dict(engine="batch", use_bounds=1, sync_rounds=1),
     "batch_sync_small": dict(engine="batch", sync_rounds=1, table_log2=6, split_threshold=64),
-    # bucket opening through bulk-copied label tiles (with tiny piles, so
-    # that tiles span several bins and the rest pile is rebuilt)
+    # bucket opening through bulk-copied label tiles (tiles span several
+    # bins; narrow buckets rebuild the band from the rest pile often)
     "batch_staged": dict(engine="batch", use_bounds=1, split_staging=1),
-    "batch_staged_small": dict(engine="batch", split_staging=1, far_capacity=1024, bucket_width=20.0,
-                               block_threads=256),
+    "batch_staged_small": dict(engine="batch", split_staging=1, bucket_width=20.0, block_threads=256,
+                               table_log2=8),
     "plain": dict(engine="plain"),
     "plain_bounds": dict(engine="plain", use_bounds=1),
 }

@@ -564,10 +564,19 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
     VINE_TRY(resolve_config(g, &r.cfg, &r));
     todo = retry;
   }
+  int32_t n_failed = 0;
   for (int32_t q = 0; q < nq; ++q) {
     if (out->status) out->status[q] = status[q];
-    if (status[q] != VINE_OK && rc == VINE_OK) rc = status[q];
+    if (status[q] != VINE_OK) {
+      ++n_failed;
+      if (rc == VINE_OK) rc = status[q];
+    }
   }
+  // this call's own message (the thread's text may still hold an older one)
+  if (rc != VINE_OK)
+    set_error(std::to_string(n_failed) + " of " + std::to_string(nq) +
+              " queries failed; first status " + std::to_string(rc) +
+              (rc == VINE_ERR_CAPACITY ? " (engine capacity, also after the retry)" : ""));
   if (want_paths) {
     int64_t run = 0;
     for (int32_t q = 0; q < nq; ++q) {
@@ -577,13 +586,12 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
     out->path_offsets[nq] = run;
     if (run > out->path_capacity || out->path == nullptr) {
       if (rc == VINE_OK) rc = fail(VINE_ERR_CAPACITY, "path buffer too small (need " + std::to_string(run) + ")");
+      else set_error(vine_last_error() + std::string("; path buffer too small (need ") + std::to_string(run) + ")");
     } else {
       for (int32_t q = 0; q < nq; ++q)
         std::memcpy(out->path + out->path_offsets[q], all_paths[q].data(), sizeof(int32_t) * all_len[q]);
     }
   }
-  if (rc != VINE_OK && rc != VINE_ERR_CAPACITY) set_error("query failed with status " + std::to_string(rc));
-  if (rc == VINE_ERR_CAPACITY && g_last_error.empty()) set_error("a query exceeded engine capacity");
   return rc;
 }
 

@@ -264,6 +264,10 @@ int vine_solve_host(int32_t n, int64_t m, const int64_t *row_ptr, const int32_t 
   }
   int rc = VINE_OK;
   int64_t run = 0;
+  int32_t n_failed = 0;
+  for (int32_t q = 0; q < nq; ++q) n_failed += status[(size_t)q] != VINE_OK;
+  if (n_failed)
+    set_error(std::to_string(n_failed) + " of " + std::to_string(nq) + " queries are invalid");
   for (int32_t q = 0; q < nq; ++q) {
     const QueryOut &r = res[(size_t)q];
     out->cost[q] = r.found ? r.cost : INFINITY;

@@ -696,11 +696,17 @@ int vine_solve_labels(vine_graph *g, int32_t kind, int32_t nq, const int32_t *sr
     return fail(VINE_ERR_CUDA, std::string("variant engine failed: ") + cudaGetErrorString(cudaGetLastError()));
   }
   if (extra) std::memcpy(extra, ex.data(), sizeof(float) * 2 * nq);
-  int result = VINE_OK;
+  int result = VINE_OK, n_failed = 0;
   for (int32_t q = 0; q < nq; ++q) {
     if (out->status) out->status[q] = st[q];
-    if (st[q] != VINE_OK && result == VINE_OK) result = st[q];
+    if (st[q] != VINE_OK) {
+      ++n_failed;
+      if (result == VINE_OK) result = st[q];
+    }
   }
+  if (result != VINE_OK)
+    set_error(std::to_string(n_failed) + " of " + std::to_string(nq) +
+              " queries failed; first status " + std::to_string(result));
   if (out->path_offsets) {
     int64_t run = 0;
     for (int32_t q = 0; q < nq; ++q) {
