@@ -151,7 +151,9 @@ enum vine_stat {
                              query started on its worker                     */
   VINE_STAT_TIME_NS,      /* batch engine: the query's duration on its worker
                              in ns (device global timer)                     */
-  VINE_STAT_COUNT = 19
+  VINE_STAT_REST_ITEMS,   /* batch engine: rest-pile labels rescanned when the
+                             band was rebuilt (part of SPLIT_ITEMS)          */
+  VINE_STAT_COUNT = 20
 };
 
 /* Values of stats[VINE_STAT_ABORT_SITE]: where a failed query stopped. */

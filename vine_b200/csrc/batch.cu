@@ -792,7 +792,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
       st.n_buckets = st.n_rounds = st.n_spills = 0;
       st.n_chain_steps = 0;
       st.n_bound_rounds = st.bound_cycles = 0;
-      st.split_cycles = st.split_items = st.policy_cycles = 0;
+      st.split_cycles = st.split_items = st.policy_cycles = st.rest_items = 0;
       st.load_cycles = st.relax_cycles = 0;
       st.hist_n = 0;
       st.sink_n = 0;
@@ -1005,6 +1005,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
           }
           if (tid == 0) {
             st.split_items += rn;
+            st.rest_items += rn;
             st.rest_n = st.rest_wpos;
           }
           __syncthreads();
@@ -1193,6 +1194,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
         s[VINE_STAT_CHAIN_STEPS] = (long long)st.n_chain_steps;
         s[VINE_STAT_START_NS] = (long long)st.g0;
         s[VINE_STAT_TIME_NS] = (long long)(global_ns() - st.g0);
+        s[VINE_STAT_REST_ITEMS] = st.rest_items;
       }
     }
     __syncthreads();

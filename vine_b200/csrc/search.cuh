@@ -104,7 +104,7 @@ struct __align__(16) QueryState {
   long long n_expanded, n_relaxed, n_inserted, n_dominated, n_buckets, n_rounds, n_spills;
   unsigned long long n_chain_steps;
   long long n_bound_rounds, bound_cycles;
-  long long split_cycles, split_items, policy_cycles, load_cycles, relax_cycles;
+  long long split_cycles, split_items, policy_cycles, load_cycles, relax_cycles, rest_items;
   // arena chunk cursor: fill (low word) and end (high word) of the current
   // chunk, also updated as one 64-bit word when warps reserve concurrently
   uint32_t chunk_fill, chunk_end;
