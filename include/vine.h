@@ -190,18 +190,19 @@ typedef struct {
   int32_t *pareto_n;      /* [nq] size of the sink Pareto set                */
   int32_t pareto_stride;
   int64_t *stats;         /* [nq*VINE_STAT_COUNT] or NULL                    */
-  int32_t retried;        /* out (vine_solve): queries solved a second time,
-                             with roomier structures, after a capacity
-                             overflow                                         */
+  int32_t retried;        /* out (vine_solve): queries solved again, with
+                             roomier structures and fewer workers at once,
+                             after a capacity overflow                        */
 } vine_results;
 
 /* Solves nq queries (source src[q], sink dst[q], delay budget budget[q]) from
  * HOST buffers; copies in, runs, copies results out.  Replaces
  * cspp<c_label,c_edge>::solve (algorithm/cspp.hpp:48-53) -> RUN_CSPP
  * (algorithm/cspp.cuh:69-325), which returned nothing; this fills cost,
- * delay, path and (in Pareto mode) the sink's Pareto set.  A query whose
- * status is VINE_ERR_CAPACITY is re-run once with larger pools before the
- * call gives up.  Returns the first per-query error, or VINE_OK. */
+ * delay, path and (in Pareto mode) the sink's Pareto set.  Queries whose
+ * status is VINE_ERR_CAPACITY are re-run, up to four times, with larger
+ * piles and arena and with fewer of them running at once, before the call
+ * gives up.  Returns the first per-query error, or VINE_OK. */
 int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst,
                const float *budget, const vine_config *cfg, vine_results *out);
 

@@ -433,6 +433,7 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
   const bool want_paths = out->path_offsets != nullptr;
 
   out->retried = 0;
+  constexpr int kMaxRetries = 4;
   std::vector<int32_t> status((size_t)nq, VINE_OK);
   std::vector<int32_t> todo((size_t)nq);
   for (int32_t i = 0; i < nq; ++i) todo[i] = i;
@@ -550,16 +551,24 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
       }
       if (hst[i] == VINE_ERR_CAPACITY) retry.push_back(q);
     }
-    if (retry.empty() || attempt >= 1) break;
-    out->retried = (int32_t)retry.size();
-    // one retry with roomier per-worker structures for the overflowing queries
+    if (retry.empty() || attempt >= kMaxRetries) break;
+    if (attempt == 0) out->retried = (int32_t)retry.size();
+    // retry the overflowing queries with roomier per-worker structures: the
+    // first retry gives each of them its own worker with 8x piles and the
+    // largest label arena; later ones halve the number of workers running
+    // at once, so that fewer heavy queries share the arena (workers keep
+    // the arena chunks of their largest query)
     ++attempt;
-    r.cfg.far_capacity = std::min<int64_t>(r.cfg.far_capacity * 8, int64_t(1) << 26);
-    r.cfg.pool_labels = std::min<int64_t>(r.cfg.pool_labels * 4, (int64_t(1) << 31) - (int64_t(1) << 20));
+    if (attempt == 1) {
+      r.cfg.far_capacity = std::min<int64_t>(r.cfg.far_capacity * 8, int64_t(1) << 24);
+      r.cfg.pool_labels = (int64_t(1) << 31) - (int64_t(1) << 20);
+      r.cfg.max_workers = (int32_t)std::min<size_t>(retry.size(), 1u << 16);
+    } else {
+      r.cfg.far_capacity = std::min<int64_t>(r.cfg.far_capacity * 2, int64_t(1) << 24);
+      r.cfg.max_workers = std::max(1, std::min(r.cfg.max_workers, (int32_t)retry.size()) / 2);
+    }
     r.cfg.spill_log2 = std::min(r.cfg.spill_log2 + 3, 22);
     r.cfg.ctas_per_sm = 1;
-    // one worker per overflowing query: the larger per-worker piles then fit
-    r.cfg.max_workers = (int32_t)std::min<size_t>(retry.size(), 1u << 16);
     r.cfg.trace = 0;
     VINE_TRY(resolve_config(g, &r.cfg, &r));
     todo = retry;

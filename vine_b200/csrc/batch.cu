@@ -715,6 +715,8 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   c.nearq = P.nearq + (size_t)slot * 2 * (P.near_mask + 1u);  // uint2 entries
   c.far = P.far + (size_t)slot * P.far_cap * 4;
   c.rest = P.rest + (size_t)slot * P.rest_cap;
+  c.far_key = P.far_key + (size_t)slot * P.far_cap * 4;
+  c.rest_key = P.rest_key + (size_t)slot * P.rest_cap;
   c.sinks = P.sinklist + (size_t)slot * P.sink_cap;
   c.bt.tv = tv;
   c.bt.tw = tw;
@@ -976,12 +978,12 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
 #pragma unroll
             for (int b = 0; b < kSplitBatch; ++b) {
               const uint32_t i = base + (uint32_t)(b * G + tid);
-              if (i < rn) item[b] = stage ? ts.buf[k][b * G + tid] : c.rest[i];
+              if (i < rn) {
+                item[b] = stage ? ts.buf[k][b * G + tid] : c.rest[i];
+                f[b] = c.rest_key[i];  // stored with the label: no h lookup
+              }
             }
-#pragma unroll
-            for (int b = 0; b < kSplitBatch; ++b)
-              if (base + (uint32_t)(b * G + tid) < rn) f[b] = key_of(c, item[b].vid, item[b].d);
-            if (!stage) __syncthreads();  // the whole tile is read before it is overwritten
+            __syncthreads();  // the whole tile (labels and keys) is read before it is overwritten
 #pragma unroll
             for (int b = 0; b < kSplitBatch; ++b) {
               if (base + (uint32_t)(b * G + tid) >= rn) break;
@@ -997,6 +999,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
                 } else {
                   const uint32_t w = warp_agg_inc(&st.rest_wpos);
                   c.rest[w] = item[b];
+                  c.rest_key[w] = f[b];
                   atomicMin(&st.rest_min_bits, __float_as_uint(f[b]));
                 }
               }
@@ -1047,8 +1050,10 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
             break;
           }
           Label item[kSplitBatch];
+          float fk[kSplitBatch];
           VView sv[kSplitBatch];
           int bj[kSplitBatch];
+          const float hi_open = bucket_hi(st);
 #pragma unroll
           for (int b = 0; b < kSplitBatch; ++b) {
             const uint32_t i = base + (uint32_t)(b * G + tid);
@@ -1057,19 +1062,30 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
               int j = 0;
               while (j < last && st.bin_pre[j + 1] <= i) ++j;
               bj[b] = j;
-              item[b] = stage ? ts.buf[k][b * G + tid]
-                              : c.far[(size_t)j * (size_t)P.bin_cap + (i - st.bin_pre[j])];
+              const size_t at = (size_t)j * (size_t)P.bin_cap + (i - st.bin_pre[j]);
+              item[b] = stage ? ts.buf[k][b * G + tid] : c.far[at];
+              fk[b] = c.far_key[at];
             }
           }
+          // only labels entering the bucket need their vertex's state
 #pragma unroll
           for (int b = 0; b < kSplitBatch; ++b)
-            if (base + (uint32_t)(b * G + tid) < fn) sv[b] = c.view(item[b].vid);
-          if (!stage) __syncthreads();  // the whole tile is read before it is overwritten
+            if (base + (uint32_t)(b * G + tid) < fn && fk[b] < hi_open) sv[b] = c.view(item[b].vid);
+          __syncthreads();  // the whole tile (labels and keys) is read before it is overwritten
+          const float inc_d =
+              key_d(*reinterpret_cast<volatile unsigned long long *>(&st.inc_key));
 #pragma unroll
           for (int b = 0; b < kSplitBatch; ++b) {
             if (base + (uint32_t)(b * G + tid) >= fn) break;
             const Label &it = item[b];
-            if (offer_with(c, it.vid, it.d, it.dl, (uint32_t)it.parent, true, sv[b])) {
+            bool stay;
+            if (fk[b] < hi_open) {
+              stay = offer_with(c, it.vid, it.d, it.dl, (uint32_t)it.parent, true, sv[b]);
+            } else {
+              // beyond the bucket: stays unless the incumbent beats its key
+              stay = !(P.mode == VINE_MODE_OPTIMAL && fk[b] > inc_d);
+            }
+            if (stay) {
               // stays in its bin (compacted in place)
               namespace cg = cooperative_groups;
               cg::coalesced_group act = cg::coalesced_threads();
@@ -1077,8 +1093,10 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
               uint32_t wb = 0;
               if (grp.thread_rank() == 0) wb = atomicAdd(&st.bin_wpos[bj[b]], grp.size());
               const uint32_t w = grp.shfl(wb, 0) + grp.thread_rank();
-              c.far[(size_t)bj[b] * (size_t)P.bin_cap + w] = it;
-              atomicMin(&st.bin_min[bj[b]], __float_as_uint(P.use_bounds ? it.d + sv[b].hlen : it.d));
+              const size_t at = (size_t)bj[b] * (size_t)P.bin_cap + w;
+              c.far[at] = it;
+              c.far_key[at] = fk[b];
+              atomicMin(&st.bin_min[bj[b]], __float_as_uint(fk[b]));
             }
           }
           __syncthreads();  // the tile's arena allocations end before the next reservation
@@ -1234,6 +1252,8 @@ void BatchWorkspace::release() {
   cudaFree(bctr);
   cudaFree(next);
   cudaFree(rest);
+  cudaFree(far_key);
+  cudaFree(rest_key);
   cudaFree(chunks);
   cudaFree(path_arena);
   cudaFree(path_start);
@@ -1262,8 +1282,10 @@ static int ensure_batch_workspace(vine_graph *g, const Resolved &r, int32_t nq) 
     // the forward band: kBins bins sharing 4 x far_capacity labels (the
     // reverse bound searches use the first far_capacity labels as one pile)
     VINE_CUDA_TRY(cudaMalloc(&w.far, sizeof(Label) * (size_t)c.far_capacity * 4 * r.slots));
+    VINE_CUDA_TRY(cudaMalloc(&w.far_key, sizeof(float) * (size_t)c.far_capacity * 4 * r.slots));
     w.rest_cap = 4 * c.far_capacity;
     VINE_CUDA_TRY(cudaMalloc(&w.rest, sizeof(Label) * (size_t)w.rest_cap * r.slots));
+    VINE_CUDA_TRY(cudaMalloc(&w.rest_key, sizeof(float) * (size_t)w.rest_cap * r.slots));
     w.max_chunks = 4096;
     VINE_CUDA_TRY(cudaMalloc(&w.chunks, sizeof(uint2) * (size_t)w.max_chunks * r.slots));
     VINE_CUDA_TRY(cudaMalloc(&w.sinklist, sizeof(uint32_t) * (size_t)sink_cap * r.slots));
@@ -1360,6 +1382,8 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.far_cap = w.far_cap;
   P.rest = w.rest;
   P.rest_cap = w.rest_cap;
+  P.far_key = w.far_key;
+  P.rest_key = w.rest_key;
   P.band_mult = c.band_mult;
   P.chunks = w.chunks;
   P.max_chunks = w.max_chunks;

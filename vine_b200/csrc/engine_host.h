@@ -31,6 +31,8 @@ struct BatchWorkspace {
   uint32_t *bctr = nullptr;     // per worker bucket counter
   uint32_t *next = nullptr;     // arena-parallel chain links
   Label *rest = nullptr;        // per worker rest pile
+  float *far_key = nullptr;     // keys beside the band bins
+  float *rest_key = nullptr;    // keys beside the rest pile
   int64_t rest_cap = 0;
   uint2 *chunks = nullptr;      // per worker arena chunk lists
   int max_chunks = 0;

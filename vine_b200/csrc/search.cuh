@@ -52,6 +52,8 @@ struct SearchParams {
   int64_t far_cap;
   Label *rest;       // keys >= band_hi
   int64_t rest_cap;
+  float *far_key;    // key f = d + h(v) of every band / rest pile entry (the
+  float *rest_key;   // key is fixed for a query, so rescans need no h lookup)
   int band_mult;     // band width in bucket widths
   uint2 *chunks;     // per worker: arena chunks (base, size) kept across queries
   int max_chunks;
@@ -183,6 +185,8 @@ struct Ctx {
   uint32_t *nearq;
   Label *far;
   Label *rest;
+  float *far_key = nullptr;   // keys beside the band bins (batch engine)
+  float *rest_key = nullptr;  // keys beside the rest pile (batch engine)
   uint32_t *sinks;
   uint32_t c_dominated = 0, c_near = 0, c_far = 0, c_spills = 0, c_candidates = 0;
   // async mode: arena slots come from this warp's slab (slab_fill points at
@@ -395,7 +399,9 @@ __device__ __forceinline__ bool push_bin(Ctx &c, const Label &l, float f) {
   if (grp.thread_rank() == 0) base = atomicAdd(&st.bin_n[j], grp.size());
   const uint32_t pos = grp.shfl(base, 0) + grp.thread_rank();
   if (pos >= (uint64_t)c.P.bin_cap) return false;
-  c.far[(size_t)j * (size_t)c.P.bin_cap + pos] = l;
+  const size_t at = (size_t)j * (size_t)c.P.bin_cap + pos;
+  c.far[at] = l;
+  c.far_key[at] = f;
   atomicMin(&st.bin_min[j], __float_as_uint(f));
   return true;
 }
@@ -420,6 +426,7 @@ __device__ __forceinline__ void push_far(Ctx &c, const Label &l, float f) {
       return;
     }
     c.rest[pos] = l;
+    if (c.rest_key) c.rest_key[pos] = f;
     atomicMin(&st.rest_min_bits, __float_as_uint(f));
   }
 }
@@ -688,12 +695,12 @@ __device__ __forceinline__ float reverse_dist(const Ctx &c, int which, int v) {
 
 
 // Scheduler step at a bucket boundary, run by one warp.  Chooses the width
-// and split threshold of the next bucket; records a trace row (the features
-// seen when the finished bucket was opened, its width and its outcome) when
-// tracing is on.  Policies: fixed width; AR(3) forecast of the bucket size
-// (after algorithm/cspp.cuh:254-284); the learned MLP, whose outputs are
-// clamped (any positive width keeps the search exact), with the AR rule as
-// fallback when it returns a non-finite value.
+// of the next bucket; records a trace row (the features seen when the
+// finished bucket was opened, its width and its outcome) when tracing is on.
+// Policies: fixed width; AR(3) forecast of the bucket size (after
+// algorithm/cspp.cuh:254-284); the learned MLP, which scales the AR rule's
+// width when its gate output says that pays (clamped: any positive width
+// keeps the search exact), with the AR rule as fallback.
 __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
   const int lane = threadIdx.x & 31;
   if (lane == 0) {
@@ -768,13 +775,13 @@ __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
     mlp_forward_warp(P.mlp, st.x, st.mh, st.y);
     if (lane == 0) {
       const float y0 = st.y[0], y1 = st.y[1];
-      if (isfinite(y0) && isfinite(y1)) {
-        // the network scales the AR rule's width for this bucket, within the
-        // range of multipliers it was trained on (2^-1.5 .. 2^1.5)
+      // y1 is a gate: the network's estimate that leaving the AR rule's
+      // width pays for this query.  Only then does y0 scale that width for
+      // this bucket, within the range of multipliers it was trained on
+      // (2^-1.5 .. 2^1.5); otherwise, and for non-finite outputs, the AR
+      // rule's width stands.
+      if (isfinite(y0) && isfinite(y1) && y1 > 0.5f)
         st.width = st.ar_width * exp2f(fminf(fmaxf(y0, -1.5f), 1.5f));
-        const float lc = fminf(fmaxf(y1, 5.0f), log2f((float)P.round_cap));
-        st.split_cap = max(32, min(P.round_cap, (int)exp2f(lc)));
-      }
     }
     __syncwarp();
   }

@@ -9,20 +9,30 @@ rule's width for the next bucket by 2^y (y clamped to [-1.5, 1.5]) from 16
 frontier statistics.  It only changes how work is grouped into buckets, so
 answers stay exact whatever it predicts.
 
-Training data comes from the plain method itself: the engine runs a query set
+Training data comes from the plain method itself: the engine runs query sets
 under the AR policy with every global width multiplier in SCALES
 (vine_config.ar_scale), with tracing on.  Each trace row holds the 16
 features the scheduler saw when a bucket was opened.  For every query the
-multiplier with the fewest SM cycles (VINE_STAT_CYCLES) is its label; every
-trace row of that query, from every run, becomes one training example
-(features -> log2(best multiplier)).  Rows from all runs keep the network
-from reading the answer off the width feature.  Training runs on the GPU
-through libvine's own forward/backward and Adam kernels.
+multiplier with the fewest SM cycles (VINE_STAT_CYCLES) is its label, kept
+at the AR rule's own width (1) unless another saves at least MARGIN of the
+query's cycles; every trace row of that query, from every run, becomes one
+training example: features -> (log2(best multiplier), gate), gate = 1 when
+the best multiplier is not the AR rule's.  The kernel applies the first
+output only where the second says the departure pays: a network that
+strays on a query it does not know falls back to the AR rule there (an
+ungated network made a few mid-sized queries several times slower, and
+those, started late in the longest-first order, stretched the batch).
+Rows from all runs keep the network from reading the answer off the width
+feature.  Training runs on the GPU through libvine's own forward/backward
+and Adam kernels.
 
-Usage: ``python -m vine_b200.scheduler [--train-config 5] [--eval-config 5]``
-(training queries come from their own query seed, so the evaluation batch
-is held out).
-writes vine_b200/models/scheduler_mlp.npy and scheduler_mlp.json.
+Usage: ``python -m vine_b200.scheduler [--train-configs 1,2,5] [--eval-configs 5,3]``
+Training traces come from the 100x100 grid (config 1), the 264k-vertex road
+graph's random pairs (config 2) and a hop-sampled batch on the same graph
+with its own query seed (config 5); evaluation runs on a held-out 4096-query
+batch (config 5, another seed) and on the 1.5M-vertex anti-correlated road
+graph (config 3).  Writes vine_b200/models/scheduler_mlp.npy and
+scheduler_mlp.json.
 """
 from __future__ import annotations
 
@@ -37,6 +47,7 @@ from . import api as v
 
 SCALES = (0.35, 0.5, 0.7, 1.0, 1.4, 2.0, 2.8)  # multipliers on the AR width
 BASE_MULT = 0.3          # initial bucket width / mean arc length
+MARGIN = 0.05            # a multiplier other than 1 must save this share of a query's cycles
 TABLE_LOG2 = 13
 MODEL_DIR = Path(__file__).resolve().parent / "models"
 MODEL_NPY = MODEL_DIR / "scheduler_mlp.npy"
@@ -68,15 +79,15 @@ def collect(graph: v.Graph, src, dst, budget, mean_len: float):
 
 
 def make_dataset(cycles, traces, settings, rows_per_setting: int = 200000, seed: int = 0,
-                 margin: float = 0.05):
-    """Features of every trace row -> log2 of the best multiplier of the
-    row's query (second output: a constant split target, unused by the
-    default asynchronous expansion).  Rows are drawn with probability
-    proportional to their query's cost (cycles per row of the query), so the
-    heavy queries that decide a batch's running time dominate the fit.
-    A query keeps the AR rule's own width (multiplier 1) unless another
-    multiplier saves at least `margin` of its cycles, so the network departs
-    from the rule it refines only where that clearly pays."""
+                 margin: float = MARGIN):
+    """Features of every trace row -> (log2 of the best multiplier of the
+    row's query, gate).  A query keeps the AR rule's own width (multiplier
+    1, gate 0) unless another multiplier saves at least `margin` of its
+    cycles (gate 1), so the network departs from the rule it refines only
+    where that clearly pays.  Half of the rows are drawn with probability
+    proportional to their query's cost (the heavy queries decide most of a
+    batch's time), half uniformly over queries (so the light and mid-sized
+    ones, which run late in a longest-first batch, are learnt too)."""
     best = np.argmin(cycles, axis=0)
     ar = settings.index(1.0)
     keep_ar = cycles[best, np.arange(cycles.shape[1])] > (1.0 - margin) * cycles[ar]
@@ -88,14 +99,16 @@ def make_dataset(cycles, traces, settings, rows_per_setting: int = 200000, seed:
         if tr.shape[0] == 0:
             continue
         q = tr[:, 16].astype(np.int64)
-        rows_of_q = np.bincount(q, minlength=cycles.shape[1]).astype(np.float64)
-        p = qcost[q] / np.maximum(rows_of_q[q], 1.0)
-        p = p / p.sum()
+        rows_of_q = np.maximum(np.bincount(q, minlength=cycles.shape[1]).astype(np.float64), 1.0)
+        p_cost = qcost[q] / rows_of_q[q]
+        p_query = 1.0 / rows_of_q[q]
+        p = 0.5 * p_cost / p_cost.sum() + 0.5 * p_query / p_query.sum()
         tr = tr[rng.choice(tr.shape[0], min(rows_per_setting, 4 * tr.shape[0]), replace=True, p=p)]
         q = tr[:, 16].astype(np.int64)
         sc = np.array([settings[b] for b in best[q]], np.float32)
+        gate = (best[q] != ar).astype(np.float32)
         xs.append(tr[:, :16])
-        ys.append(np.stack([np.log2(sc), np.full_like(sc, 10.0)], axis=1))
+        ys.append(np.stack([np.log2(sc), gate], axis=1))
     x = np.concatenate(xs).astype(np.float32)
     y = np.concatenate(ys).astype(np.float32)
     ok = np.isfinite(x).all(1) & np.isfinite(y).all(1)
@@ -155,10 +168,11 @@ def load(device: int = 0):
     return v.MLP(device=device, params=np.load(MODEL_NPY)), meta
 
 
-def _evaluate_batch(a, mlp):
-    """Fixed / AR / network on a whole batch drawn with its own query seed."""
-    over = {"n_pairs": a.eval_queries, "query_seed": a.eval_seed} if a.eval_config == 5 else {}
-    ev = v.Workload.generate(a.eval_config, **over)
+def _evaluate_batch(a, mlp, config: int):
+    """Fixed / AR / network on a whole batch (config 5: drawn with its own
+    query seed, held out from training and from the bench batch)."""
+    over = {"n_pairs": a.eval_queries, "query_seed": a.eval_seed} if config == 5 else {}
+    ev = v.Workload.generate(config, **over)
     n = len(ev.src)
     ge = ev.graph()
     res = evaluate(ge, ev.src, ev.dst, ev.budget, float(ev.len.mean()), mlp)
@@ -166,13 +180,24 @@ def _evaluate_batch(a, mlp):
     return res, n
 
 
+def _evaluate_all(a, mlp) -> dict:
+    out = {}
+    for cfg in a.eval_configs:
+        res, n = _evaluate_batch(a, mlp, cfg)
+        out[str(cfg)] = dict(res, queries=n)
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--train-config", type=int, default=5)
-    ap.add_argument("--train-queries", type=int, default=1024)
+    ap.add_argument("--train-configs", default="1,2,5",
+                    help="workloads whose traces train the network")
+    ap.add_argument("--train-queries", type=int, default=1024,
+                    help="queries of the config-5 training batch")
     ap.add_argument("--train-seed", type=int, default=0x7EA1,
                     help="query seed of the training batch (the bench batch uses the default seed)")
-    ap.add_argument("--eval-config", type=int, default=5)
+    ap.add_argument("--eval-configs", default="5,3",
+                    help="held-out evaluation workloads (the first one decides `mlp_faster`)")
     ap.add_argument("--eval-queries", type=int, default=4096)
     ap.add_argument("--eval-seed", type=int, default=0xE7A1,
                     help="query seed of the evaluation batch (neither the training nor the bench batch)")
@@ -181,43 +206,63 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--out", default=None, help="write the evaluation JSON here")
     a = ap.parse_args(argv)
+    a.eval_configs = [int(x) for x in a.eval_configs.split(",") if x]
+    a.train_configs = [int(x) for x in a.train_configs.split(",") if x]
 
     t0 = time.time()
     if a.eval_only:
         mlp, meta = load()
         if mlp is None:
             raise SystemExit("no trained scheduler to evaluate")
-        res, n = _evaluate_batch(a, mlp)
-        meta.update({"eval_config": a.eval_config, "eval_queries": n, "eval_seed": a.eval_seed,
-                     "eval": res})
+        ev = _evaluate_all(a, mlp)
+        first = ev[str(a.eval_configs[0])]
+        meta.update({"eval_config": a.eval_configs[0], "eval_queries": first["queries"],
+                     "eval_seed": a.eval_seed,
+                     "eval": {k: v_ for k, v_ in first.items() if k != "queries"},
+                     "eval_by_config": ev})
         MODEL_JSON.write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
         text = json.dumps(meta, indent=1, sort_keys=True)
         if a.out:
             Path(a.out).write_text(text + "\n")
         print(text)
         return
-    over = {"n_pairs": a.train_queries, "query_seed": a.train_seed} if a.train_config == 5 else {}
-    wl = v.Workload.generate(a.train_config, **over)
-    mean_len = float(wl.len.mean())
-    g = wl.graph()
-    cycles, traces, settings = collect(g, wl.src, wl.dst, wl.budget, mean_len)
-    x, y = make_dataset(cycles, traces, settings)
-    best = np.argmin(cycles, axis=0)
-    hist = {str(settings[k]): int((best == k).sum()) for k in range(len(settings))}
-    mlp, loss0, loss = train(x, y, epochs=a.epochs)
-    static_best = int(np.argmin(cycles.sum(1)))
-    g.close()
-
-    res, n = _evaluate_batch(a, mlp)
-    meta = {"base_mult": BASE_MULT, "table_log2": TABLE_LOG2, "block_threads": 512,
-            "train_config": a.train_config, "rows": int(x.shape[0]),
-            "loss_initial": loss0, "loss_final": loss, "epochs": a.epochs,
-            "best_setting_histogram": hist,
+    xs, ys, per_config = [], [], {}
+    for tc in a.train_configs:
+        over = {"n_pairs": a.train_queries, "query_seed": a.train_seed} if tc == 5 else {}
+        wl = v.Workload.generate(tc, **over)
+        g = wl.graph()
+        cycles, traces, settings = collect(g, wl.src, wl.dst, wl.budget, float(wl.len.mean()))
+        g.close()
+        x, y = make_dataset(cycles, traces, settings)
+        xs.append(x)
+        ys.append(y)
+        best = np.argmin(cycles, axis=0)
+        static_best = int(np.argmin(cycles.sum(1)))
+        per_config[str(tc)] = {
+            "queries": int(len(wl.src)), "rows": int(x.shape[0]),
+            "best_setting_histogram": {str(settings[k]): int((best == k).sum())
+                                       for k in range(len(settings))},
+            "gate_share": float(y[:, 1].mean()),
             "best_static_setting": settings[static_best],
             "oracle_best_per_query_cycles": float(cycles.min(0).sum()),
             "best_static_cycles": float(cycles[static_best].sum()),
-            "eval_config": a.eval_config, "eval_queries": n, "eval_seed": a.eval_seed,
-            "eval": res,
+            "ar_cycles": float(cycles[settings.index(1.0)].sum())}
+    x = np.concatenate(xs)
+    y = np.concatenate(ys)
+    perm = np.random.default_rng(1).permutation(x.shape[0])
+    x, y = x[perm], y[perm]
+    mlp, loss0, loss = train(x, y, epochs=a.epochs)
+
+    ev = _evaluate_all(a, mlp)
+    first = ev[str(a.eval_configs[0])]
+    meta = {"base_mult": BASE_MULT, "table_log2": TABLE_LOG2, "block_threads": 512,
+            "margin": MARGIN, "train_configs": a.train_configs, "rows": int(x.shape[0]),
+            "loss_initial": loss0, "loss_final": loss, "epochs": a.epochs,
+            "training": per_config,
+            "eval_config": a.eval_configs[0], "eval_queries": first["queries"],
+            "eval_seed": a.eval_seed,
+            "eval": {k: v_ for k, v_ in first.items() if k != "queries"},
+            "eval_by_config": ev,
             "seconds": time.time() - t0}
     save(mlp, meta)
     text = json.dumps(meta, indent=1, sort_keys=True)
