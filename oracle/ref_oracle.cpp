@@ -378,7 +378,7 @@ class MaxLabel {
   }
 };
 
-// Network QoS (include/label.hpp:367-463): d adds lengths, delay is the
+// Network QoS (include/label.hpp:382-464): d adds lengths, delay is the
 // bottleneck bandwidth min(delay, arc delay), starting at 21474836;
 // constraint bandwidth >= L.
 class QosLabel {
@@ -406,7 +406,7 @@ class c_constraint<HopLabel> {
   }
 };
 
-// include/constraint.hpp:51-80
+// include/constraint.hpp:50-80
 template <>
 class c_constraint<MaxLabel> {
  public:
@@ -420,7 +420,7 @@ class c_constraint<MaxLabel> {
   }
 };
 
-// include/constraint.hpp:161-187
+// include/constraint.hpp:162-186
 template <>
 class c_constraint<QosLabel> {
  public:

@@ -571,6 +571,7 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
     r.cfg.ctas_per_sm = 1;
     r.cfg.trace = 0;
     VINE_TRY(resolve_config(g, &r.cfg, &r));
+    r.chunk_log2 = 20;  // 4096 chunks of 2^20 labels per worker: room for any query the arena holds
     todo = retry;
   }
   int32_t n_failed = 0;

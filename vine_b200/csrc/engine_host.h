@@ -148,6 +148,9 @@ struct Resolved {
   int slots;
   float width0;
   int round_cap;
+  int chunk_log2 = 16;  // arena chunk size a worker takes at a time (2^16 labels;
+                        // capacity retries use larger chunks, since a worker
+                        // holds at most 4096 of them)
 };
 
 int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out);

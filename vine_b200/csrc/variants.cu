@@ -42,7 +42,7 @@ struct __align__(16) VLabel {
   uint32_t pad;
 };
 
-constexpr float kQosStart = 21474836.0f;  // the reference's initial bandwidth (label.hpp:380-384)
+constexpr float kQosStart = 21474836.0f;  // the reference's initial bandwidth (include/label.hpp:396-399)
 
 template <int K>
 struct Ops;
@@ -73,7 +73,7 @@ struct Ops<VINE_LABEL_HOP> {
   static constexpr int kKey = 3;
   __device__ static void source(VLabel &l) { l.r0 = l.r1 = l.r2 = 0.0f; }
   __device__ static void expand(const VLabel &a, float len, float dly, VLabel &c) {
-    c.d = a.d + len;  // include/label.hpp:89-97
+    c.d = a.d + len;  // include/label.hpp:88-97
     c.r0 = a.r0 + dly;
     c.r1 = a.r1 + 1.0f;
     c.r2 = 0.0f;
@@ -96,7 +96,7 @@ struct Ops<VINE_LABEL_MAXCOST> {
   static constexpr int kKey = 4;
   __device__ static void source(VLabel &l) { l.r0 = l.r1 = l.r2 = 0.0f; }
   __device__ static void expand(const VLabel &a, float len, float dly, VLabel &c) {
-    c.d = a.d + len;  // include/label.hpp:150-159
+    c.d = a.d + len;  // include/label.hpp:151-160
     c.r0 = a.r0 + dly;
     c.r1 = a.r1 + 1.0f;
     c.r2 = fmaxf(a.r2, len);
@@ -105,7 +105,7 @@ struct Ops<VINE_LABEL_MAXCOST> {
     return a.d <= b.d && a.r0 <= b.r0 && a.r1 <= b.r1 && a.r2 <= b.r2;  // :161-166
   }
   __device__ static bool feasible(const VLabel &l, float L, float H, float M) {
-    return !(l.r0 > L || l.r1 > H || l.r2 > M);  // include/constraint.hpp:72-78
+    return !(l.r0 > L || l.r1 > H || l.r2 > M);  // include/constraint.hpp:73-79
   }
   __device__ static void key(const VLabel &l, float *k) {
     k[0] = l.d;
@@ -123,12 +123,12 @@ struct Ops<VINE_LABEL_QOS> {
     l.r1 = l.r2 = 0.0f;
   }
   __device__ static void expand(const VLabel &a, float len, float dly, VLabel &c) {
-    c.d = a.d + len;  // include/label.hpp:417-425
+    c.d = a.d + len;  // include/label.hpp:424-431
     c.r0 = fminf(a.r0, dly);
     c.r1 = c.r2 = 0.0f;
   }
   __device__ static bool dominates(const VLabel &a, const VLabel &b) {
-    return a.d <= b.d && a.r0 >= b.r0;  // include/label.hpp:436-441
+    return a.d <= b.d && a.r0 >= b.r0;  // include/label.hpp:445-450
   }
   __device__ static bool feasible(const VLabel &l, float L, float, float) {
     return !(l.r0 < L);  // include/constraint.hpp:180-182
