@@ -1000,7 +1000,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
                   const uint32_t w = warp_agg_inc(&st.rest_wpos);
                   c.rest[w] = item[b];
                   c.rest_key[w] = f[b];
-                  warp_agg_min(&st.rest_min_bits, __float_as_uint(f[b]));
+                  atomicMin(&st.rest_min_bits, __float_as_uint(f[b]));
                 }
               }
             }
@@ -1096,7 +1096,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
               const size_t at = (size_t)bj[b] * (size_t)P.bin_cap + w;
               c.far[at] = it;
               c.far_key[at] = fk[b];
-              group_min(grp, &st.bin_min[bj[b]], __float_as_uint(fk[b]));
+              atomicMin(&st.bin_min[bj[b]], __float_as_uint(fk[b]));
             }
           }
           __syncthreads();  // the tile's arena allocations end before the next reservation

@@ -17,7 +17,6 @@
 #pragma once
 
 #include <cooperative_groups.h>
-#include <cooperative_groups/reduce.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -157,24 +156,6 @@ __device__ __forceinline__ uint32_t warp_agg_inc(uint32_t *ctr) {
   if (grp.thread_rank() == 0) base = atomicAdd(ctr, (uint32_t)grp.size());
   base = grp.shfl(base, 0);
   return base + (uint32_t)grp.thread_rank();
-}
-
-// Lowers *addr to the smallest v of the converged lanes with one shared or
-// global atomic per group instead of one per lane (non-negative floats are
-// passed as their bit patterns, which order like the values).
-__device__ __forceinline__ void warp_agg_min(uint32_t *addr, uint32_t v) {
-  namespace cg = cooperative_groups;
-  cg::coalesced_group grp = cg::coalesced_threads();
-  const uint32_t m = cg::reduce(grp, v, cg::less<uint32_t>());
-  if (grp.thread_rank() == 0) atomicMin(addr, m);
-}
-
-// The same for the lanes of a labelled partition (one bin per group).
-__device__ __forceinline__ void group_min(const cooperative_groups::coalesced_group &grp,
-                                          uint32_t *addr, uint32_t v) {
-  namespace cg = cooperative_groups;
-  const uint32_t m = cg::reduce(grp, v, cg::less<uint32_t>());
-  if (grp.thread_rank() == 0) atomicMin(addr, m);
 }
 
 // Thread -> work-item order that deals consecutive items to different warps

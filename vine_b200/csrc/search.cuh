@@ -398,14 +398,12 @@ __device__ __forceinline__ bool push_bin(Ctx &c, const Label &l, float f) {
   uint32_t base = 0;
   if (grp.thread_rank() == 0) base = atomicAdd(&st.bin_n[j], grp.size());
   const uint32_t pos = grp.shfl(base, 0) + grp.thread_rank();
-  const bool fits = pos < (uint64_t)c.P.bin_cap;
-  if (fits) {
-    const size_t at = (size_t)j * (size_t)c.P.bin_cap + pos;
-    c.far[at] = l;
-    c.far_key[at] = f;
-  }
-  group_min(grp, &st.bin_min[j], fits ? __float_as_uint(f) : 0xffffffffu);
-  return fits;
+  if (pos >= (uint64_t)c.P.bin_cap) return false;
+  const size_t at = (size_t)j * (size_t)c.P.bin_cap + pos;
+  c.far[at] = l;
+  c.far_key[at] = f;
+  atomicMin(&st.bin_min[j], __float_as_uint(f));
+  return true;
 }
 
 __device__ __forceinline__ void push_far(Ctx &c, const Label &l, float f) {
@@ -423,13 +421,13 @@ __device__ __forceinline__ void push_far(Ctx &c, const Label &l, float f) {
     atomicMin(&st.far_min_bits, __float_as_uint(f));
   } else {
     const uint32_t pos = warp_agg_inc(&st.rest_n);
-    warp_agg_min(&st.rest_min_bits, __float_as_uint(f));
     if (pos >= (uint64_t)c.P.rest_cap) {
       fail_query(st, VINE_ERR_CAPACITY, kSiteRest);
       return;
     }
     c.rest[pos] = l;
     if (c.rest_key) c.rest_key[pos] = f;
+    atomicMin(&st.rest_min_bits, __float_as_uint(f));
   }
 }
 
