@@ -105,8 +105,8 @@ typedef struct {
   int32_t sync_rounds;     /* batch engine: 1 = block-synchronous expansion
                               rounds of at most split_threshold labels;
                               0 = warps pull labels from the bucket's queue */
-  int32_t band_mult;       /* batch engine: near far-pile band, in bucket
-                              widths (0 = 8)                                  */
+  int32_t band_mult;       /* batch engine: near far-pile band (64 key bins),
+                              in bucket widths (0 = 16)                       */
   float ar_scale;          /* AR / MLP policies: multiplier applied to the AR
                               rule's width (0 = 1)                            */
   int32_t wait_limit;      /* every bounded device wait (lock attempts, polls

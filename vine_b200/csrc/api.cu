@@ -155,7 +155,7 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
   if (!(c.bucket_width >= 0.0f) || !std::isfinite(c.bucket_width))
     return fail(VINE_ERR_INVALID, "bucket_width must be finite and >= 0");
   if (c.max_workers < 0) return fail(VINE_ERR_INVALID, "max_workers must be >= 0");
-  if (c.band_mult == 0) c.band_mult = 8;
+  if (c.band_mult == 0) c.band_mult = 16;
   if (c.ar_scale == 0.0f) c.ar_scale = 1.0f;
   if (!(c.ar_scale >= 1.0f / 64.0f && c.ar_scale <= 64.0f))
     return fail(VINE_ERR_INVALID, "ar_scale in [1/64, 64]");

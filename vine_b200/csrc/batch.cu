@@ -18,7 +18,7 @@
 //   * settled delay -- one float per vertex summarising finished buckets
 //   * near queue    -- ring of (arena index, vertex) still to expand in this
 //                      bucket, published to the warps in reservation order
-//   * far band/rest -- labels beyond the bucket: a band of 16 key bins, so that
+//   * far band/rest -- labels beyond the bucket: a band of 64 key bins, so that
 //                      opening a bucket scans only the bins below its key, and
 //                      a rest pile behind it (the reference's DOP split /
 //                      recheck, algorithm/cspp.cuh:179-216,

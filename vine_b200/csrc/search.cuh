@@ -23,7 +23,7 @@ constexpr int kHist = kBurgMaxN;
 constexpr uint32_t kInfBits = 0x7f800000u;
 constexpr int kScanScratch = 40;
 constexpr long long kMaxRounds = 1ll << 26;  // hard progress bound per query
-constexpr int kBins = 16;                    // key bins of the band (binned mode)
+constexpr int kBins = 64;                    // key bins of the band (binned mode)
 constexpr long long kMaxBuckets = 1ll << 22; // hard bound on buckets per query
 
 struct SearchParams {

@@ -124,7 +124,7 @@ def train(x, y, device: int = 0, epochs: int = 30, batch: int = 512, lr: float =
 
 
 def evaluate(graph: v.Graph, src, dst, budget, mean_len: float, mlp, repeats: int = 3,
-             answers=None):
+             answers=None, warm_up: bool = True):
     """Times the batch engine under the fixed, AR and MLP policies (same base
     width); returns {policy: {ms, cycles, expanded}} and checks every arm
     returns identical costs."""
@@ -136,7 +136,8 @@ def evaluate(graph: v.Graph, src, dst, budget, mean_len: float, mlp, repeats: in
     if mlp is not None:
         arms["mlp"] = base_config(mean_len, policy="mlp", mlp=mlp)
     for name, cfg in arms.items():
-        v.solve(graph, src, dst, budget, cfg, paths=False)  # warm-up
+        if warm_up:
+            v.solve(graph, src, dst, budget, cfg, paths=False)
         times = []
         for _ in range(repeats):
             torch.cuda.synchronize()
@@ -147,7 +148,9 @@ def evaluate(graph: v.Graph, src, dst, budget, mean_len: float, mlp, repeats: in
             ref = (r.cost.copy(), r.found.copy())
         same = bool(np.array_equal(r.found, ref[1]) and
                     np.array_equal(np.where(r.found == 1, r.cost, 0), np.where(ref[1] == 1, ref[0], 0)))
-        out[name] = {"ms": float(np.median(times)), "cycles": float(r.stats[:, STAT_CYCLES].sum()),
+        out[name] = {"ms": float(np.median(times)), "ms_all": [round(t, 1) for t in times],
+                     "retried": int(r.retried),
+                     "cycles": float(r.stats[:, STAT_CYCLES].sum()),
                      "cycles_max": float(r.stats[:, STAT_CYCLES].max()),
                      "expanded": int(r.stats[:, 0].sum()), "rounds": int(r.stats[:, 5].sum()),
                      "same_answers": same}
@@ -175,7 +178,10 @@ def _evaluate_batch(a, mlp, config: int):
     ev = v.Workload.generate(config, **over)
     n = len(ev.src)
     ge = ev.graph()
-    res = evaluate(ge, ev.src, ev.dst, ev.budget, float(ev.len.mean()), mlp)
+    # the 1.5M-vertex batch takes minutes per arm: one timed run each
+    heavy = config == 3
+    res = evaluate(ge, ev.src, ev.dst, ev.budget, float(ev.len.mean()), mlp,
+                   repeats=1 if heavy else 3, warm_up=not heavy)
     ge.close()
     return res, n
 
