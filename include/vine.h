@@ -153,7 +153,11 @@ enum vine_stat {
                              in ns (device global timer)                     */
   VINE_STAT_REST_ITEMS,   /* batch engine: rest-pile labels rescanned when the
                              band was rebuilt (part of SPLIT_ITEMS)          */
-  VINE_STAT_COUNT = 20
+  VINE_STAT_IDLE_CYCLES,  /* batch engine: warp-cycles (summed over warps) of
+                             polling an empty bucket queue                   */
+  VINE_STAT_PUBLISH_CYCLES,/* batch engine: warp-cycles waiting to publish
+                             queue entries in reservation order              */
+  VINE_STAT_COUNT = 22
 };
 
 /* Values of stats[VINE_STAT_ABORT_SITE]: where a failed query stopped. */

@@ -36,8 +36,8 @@ POLICY_FIXED, POLICY_AR, POLICY_MLP = 0, 1, 2
 STAT_NAMES = ["expanded", "relaxed", "inserted", "dominated", "buckets", "rounds", "spills",
               "cycles", "abort_site", "bound_rounds", "bound_cycles", "chain_steps",
               "split_cycles", "split_items", "policy_cycles", "load_cycles", "relax_cycles",
-              "start_ns", "time_ns", "rest_items"]
-STAT_COUNT = 20
+              "start_ns", "time_ns", "rest_items", "idle_cycles", "publish_cycles"]
+STAT_COUNT = 22
 STAT_CYCLES, STAT_START_NS, STAT_TIME_NS = 7, 17, 18
 STAT_ABORT_SITE = 8
 SITE_LOCK, SITE_ASYNC, SITE_TIME, SITE_RING = 7, 12, 13, 14

@@ -157,16 +157,21 @@ constexpr uint32_t kSlab = 1024;  // arena slots a warp takes at a time
 // up publishes nothing (the query is failed, and its consumers stop at the
 // abort flag before taking entries).
 __device__ __forceinline__ void publish_entries(const SearchParams &P, QueryState &st,
-                                                uint32_t base, uint32_t k) {
+                                                uint32_t base, uint32_t k,
+                                                unsigned long long *waited) {
   __threadfence_block();
   volatile uint32_t *cm = &st.near_commit;
-  long long polls = 0;
-  while (*cm != base) {
-    if (*reinterpret_cast<volatile int *>(&st.abort)) return;
-    if (++polls > P.wait_limit) {
-      fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
-      return;
+  if (*cm != base) {
+    const long long t0 = clock64();
+    long long polls = 0;
+    while (*cm != base) {
+      if (*reinterpret_cast<volatile int *>(&st.abort) || ++polls > P.wait_limit) {
+        if (!*reinterpret_cast<volatile int *>(&st.abort)) fail_query(st, VINE_ERR_TIMEOUT, kSiteAsync);
+        *waited += (unsigned long long)(clock64() - t0);
+        return;
+      }
     }
+    *waited += (unsigned long long)(clock64() - t0);
   }
   *cm = base + k;
 }
@@ -191,7 +196,7 @@ __device__ __forceinline__ void async_push(Ctx &c, bool is_near, uint32_t idx, i
     c.near_ring()[(base + rank) & P.near_mask] = make_uint2(idx, (uint32_t)v);
   }
   __syncwarp();
-  if (lane == 0) publish_entries(P, st, base, k);
+  if (lane == 0) publish_entries(P, st, base, k, &c.c_publish);
   __syncwarp();
 }
 
@@ -206,12 +211,14 @@ __device__ __forceinline__ void bucket_async(Ctx &c) {
   // reaches the limit, however long the other warps' expansions take
   long long idle = 0;
   uint32_t seen_commit = 0xffffffffu, seen_pending = 0xffffffffu;
+  uint32_t w_expanded = 0, w_relaxed = 0, w_rounds = 0;
   for (;;) {
     // ---- take up to 32 entries (fewer when the ring is short, so that the
     // ---- idle warps share the work)
     uint32_t h = 0, take = 0;
     int stop = 0;
     if (lane == 0) {
+      long long t_idle = 0;
       for (;;) {
         if (*reinterpret_cast<volatile int *>(&st.abort)) {
           stop = 1;
@@ -235,6 +242,7 @@ __device__ __forceinline__ void bucket_async(Ctx &c) {
           stop = 1;
           break;
         }
+        if (t_idle == 0) t_idle = clock64();
         if (cm != seen_commit || pend != seen_pending) {
           seen_commit = cm;
           seen_pending = pend;
@@ -251,6 +259,7 @@ __device__ __forceinline__ void bucket_async(Ctx &c) {
         }
         __nanosleep(32);
       }
+      if (t_idle) c.c_idle += (unsigned long long)(clock64() - t_idle);
     }
     if (__shfl_sync(FULL, stop, 0)) break;
     h = __shfl_sync(FULL, h, 0);
@@ -301,16 +310,10 @@ __device__ __forceinline__ void bucket_async(Ctx &c) {
     }
     const int total = __shfl_sync(FULL, incl, 31);
     const int excl = incl - deg;
-    const unsigned expanded = __ballot_sync(FULL, deg > 0);
-    if (lane == 0) {
-      const uint32_t ne = (uint32_t)__popc(expanded);
-      atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_expanded), (unsigned long long)ne);
-      atomicAdd(&st.b_expanded, ne);
-      atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_relaxed), (unsigned long long)total);
-      atomicAdd(&st.b_relaxed, (uint32_t)total);
-      atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_rounds), 1ull);
-      atomicAdd(&st.b_rounds, 1u);
-    }
+    // this bucket's counters, kept per warp and folded in once at the end
+    w_expanded += (uint32_t)__popc(__ballot_sync(FULL, deg > 0));
+    w_relaxed += (uint32_t)total;
+    w_rounds += 1u;
 
     // ---- the arcs, 32 at a time
     if (total > 0) {
@@ -363,7 +366,18 @@ __device__ __forceinline__ void bucket_async(Ctx &c) {
     __syncwarp();
     if (lane == 0) atomicSub(&st.pending, take);
   }
-  // fold the per-thread counters into the bucket statistics
+  // fold the per-warp and per-thread counters into the bucket statistics
+  if (lane == 0) {
+    atomicAdd(&st.idle_cycles, c.c_idle);
+    atomicAdd(&st.publish_cycles, c.c_publish);
+    c.c_idle = c.c_publish = 0;
+    atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_expanded), (unsigned long long)w_expanded);
+    atomicAdd(&st.b_expanded, w_expanded);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_relaxed), (unsigned long long)w_relaxed);
+    atomicAdd(&st.b_relaxed, w_relaxed);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&st.n_rounds), (unsigned long long)w_rounds);
+    atomicAdd(&st.b_rounds, w_rounds);
+  }
   atomicAdd(&st.b_dominated, c.c_dominated);
   atomicAdd(&st.b_candidates, c.c_candidates);
   atomicAdd(&st.b_spilled, c.c_spills);
@@ -395,7 +409,7 @@ __device__ __forceinline__ void async_push_vertex(Ctx &c, bool is_push, int32_t 
     c.nearq[(base + rank) & P.near_mask] = (uint32_t)u;
   }
   __syncwarp();
-  if (lane == 0) publish_entries(P, st, base, k);
+  if (lane == 0) publish_entries(P, st, base, k, &c.c_publish);
   __syncwarp();
 }
 
@@ -795,6 +809,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
       st.n_chain_steps = 0;
       st.n_bound_rounds = st.bound_cycles = 0;
       st.split_cycles = st.split_items = st.policy_cycles = st.rest_items = 0;
+      st.idle_cycles = st.publish_cycles = 0;
       st.load_cycles = st.relax_cycles = 0;
       st.hist_n = 0;
       st.sink_n = 0;
@@ -1213,6 +1228,8 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
         s[VINE_STAT_START_NS] = (long long)st.g0;
         s[VINE_STAT_TIME_NS] = (long long)(global_ns() - st.g0);
         s[VINE_STAT_REST_ITEMS] = st.rest_items;
+        s[VINE_STAT_IDLE_CYCLES] = (long long)st.idle_cycles;
+        s[VINE_STAT_PUBLISH_CYCLES] = (long long)st.publish_cycles;
       }
     }
     __syncthreads();

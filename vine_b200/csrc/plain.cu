@@ -269,6 +269,8 @@ __global__ void plain_finish_kernel(PlainArgs A, int q) {
       s[VINE_STAT_START_NS] = 0;
       s[VINE_STAT_TIME_NS] = 0;
       s[VINE_STAT_REST_ITEMS] = 0;
+      s[VINE_STAT_IDLE_CYCLES] = 0;
+      s[VINE_STAT_PUBLISH_CYCLES] = 0;
     }
   }
 }

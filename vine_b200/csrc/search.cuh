@@ -107,6 +107,7 @@ struct __align__(16) QueryState {
   unsigned long long n_chain_steps;
   long long n_bound_rounds, bound_cycles;
   long long split_cycles, split_items, policy_cycles, load_cycles, relax_cycles, rest_items;
+  unsigned long long idle_cycles, publish_cycles;
   // arena chunk cursor: fill (low word) and end (high word) of the current
   // chunk, also updated as one 64-bit word when warps reserve concurrently
   uint32_t chunk_fill, chunk_end;
@@ -189,6 +190,7 @@ struct Ctx {
   float *rest_key = nullptr;  // keys beside the rest pile (batch engine)
   uint32_t *sinks;
   uint32_t c_dominated = 0, c_near = 0, c_far = 0, c_spills = 0, c_candidates = 0;
+  unsigned long long c_idle = 0, c_publish = 0;  // warps-pull waits (lane 0 of each warp)
   // async mode: arena slots come from this warp's slab (slab_fill points at
   // its fill counter; the slab always has room for the 32 arcs in flight)
   uint32_t *slab_fill = nullptr;
