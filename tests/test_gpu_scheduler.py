@@ -52,5 +52,6 @@ def test_trained_scheduler_beats_fixed_and_matches_ar(road):
     print(f"SM cycles over {len(sel)} held-out queries: fixed {cyc['fixed']:.3e}, "
           f"AR {cyc['ar']:.3e}, trained {cyc['mlp']:.3e} "
           f"(trained/fixed {cyc['mlp'] / cyc['fixed']:.3f}, trained/AR {cyc['mlp'] / cyc['ar']:.3f})")
+    # the network does less work than both rules it is compared with
     assert cyc["mlp"] < 0.8 * cyc["fixed"]
-    assert cyc["mlp"] <= 1.05 * cyc["ar"]
+    assert cyc["mlp"] < cyc["ar"]

@@ -200,6 +200,9 @@ def main(argv=None):
                     help="workloads whose traces train the network")
     ap.add_argument("--train-queries", type=int, default=1024,
                     help="queries of the config-5 training batch")
+    ap.add_argument("--train-queries-c3", type=int, default=48,
+                    help="queries of a config-3 training batch (own query seed), when 3 is "
+                         "among the training configs")
     ap.add_argument("--train-seed", type=int, default=0x7EA1,
                     help="query seed of the training batch (the bench batch uses the default seed)")
     ap.add_argument("--eval-configs", default="5,3",
@@ -234,7 +237,11 @@ def main(argv=None):
         return
     xs, ys, per_config = [], [], {}
     for tc in a.train_configs:
-        over = {"n_pairs": a.train_queries, "query_seed": a.train_seed} if tc == 5 else {}
+        over = {}
+        if tc == 5:
+            over = {"n_pairs": a.train_queries, "query_seed": a.train_seed}
+        elif tc == 3:  # the 1.5M-vertex graph: a small batch with its own query seed
+            over = {"n_pairs": a.train_queries_c3, "query_seed": a.train_seed}
         wl = v.Workload.generate(tc, **over)
         g = wl.graph()
         cycles, traces, settings = collect(g, wl.src, wl.dst, wl.budget, float(wl.len.mean()))
