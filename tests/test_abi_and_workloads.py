@@ -160,3 +160,31 @@ def test_dropin_graph_model_builds_the_csr(tmp_path):
     assert np.array_equal(slots[:, 1].astype(np.float32), fx["len"])
     assert np.array_equal(slots[:, 2].astype(np.float32), fx["delay"])
     assert np.array_equal(slots[:, 3].astype(np.int64), np.arange(m))  # edge ids in file order
+
+
+def test_reference_arm_loads_no_engine_library(tmp_path):
+    """bench.py --impl reference times the reference's CPU solver on the same
+    seeded workload without loading the engine's library (it builds the
+    workload with the generator copy in oracle/_ref)."""
+    import json
+    import sys
+    from oracle import oracle as O
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    code = (
+        "import sys, json, types\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', '--nq', '48']\n"
+        "import bench\n"
+        "bench.main()\n"
+        "mods = [m for m in sys.modules if m.startswith('vine_b200')]\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'mods': mods, 'libvine': 'libvine.so' in maps}))\n")
+    root = Path(__file__).resolve().parents[1]
+    res = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True,
+                         timeout=600)
+    assert res.returncode == 0, res.stderr[-3000:]
+    lines = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["value"] > 0
+    check = json.loads(lines[-1])
+    assert check == {"mods": [], "libvine": False}
