@@ -177,9 +177,8 @@ enum vine_abort_site {
   VINE_SITE_ASYNC = 12,      /* a bucket-queue wait reached wait_limit        */
   VINE_SITE_TIME = 13,       /* time_limit_ms reached                         */
   VINE_SITE_RING = 14,       /* a queue entry failed its range check          */
-  VINE_SITE_TILE = 15,       /* a staged label tile's copy did not land within
+  VINE_SITE_TILE = 15        /* a staged label tile's copy did not land within
                                 wait_limit polls (the worker then stops)      */
-  VINE_SITE_DEEP = 16        /* deep pile full (labels far beyond the band)   */
 };
 
 typedef struct {

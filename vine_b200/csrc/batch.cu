@@ -564,10 +564,6 @@ __device__ void reverse_bucket_async(Ctx &c, int which, float radius) {
 // Far-pile items per thread whose loads are issued together when a bucket
 // opens (more would spill registers around the inlined insert path).
 constexpr int kSplitBatch = 2;
-// The rest pile holds keys within kDeepBands band widths past the band; the
-// deep pile holds the keys beyond, so a band rebuild rescans only the labels
-// of the next few bands.
-constexpr int kDeepBands = 8;
 
 // ------------------------------------------------- bulk-staged label tiles
 //
@@ -735,8 +731,6 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
   c.rest = P.rest + (size_t)slot * P.rest_cap;
   c.far_key = P.far_key + (size_t)slot * P.far_cap * 4;
   c.rest_key = P.rest_key + (size_t)slot * P.rest_cap;
-  c.deep = P.deep + (size_t)slot * P.rest_cap;
-  c.deep_key = P.deep_key + (size_t)slot * P.rest_cap;
   c.sinks = P.sinklist + (size_t)slot * P.sink_cap;
   c.bt.tv = tv;
   c.bt.tw = tw;
@@ -805,11 +799,6 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
       st.rest_n = 0;
       st.rest_wpos = 0;
       st.rest_min_bits = kInfBits;
-      st.deep_n = 0;
-      st.deep_wpos = 0;
-      st.deep_min_bits = kInfBits;
-      st.rest_hi = INFINITY;
-      st.rb_deep = 0;
       st.band_hi = INFINITY;
       st.near_head = st.near_tail = 0;
       st.abort = 0;
@@ -879,7 +868,6 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
           st.hi_bits = __float_as_uint(sv.hlen + P.width0);
           st.band_lo = sv.hlen;
           st.band_hi = sv.hlen + P.width0 * (float)P.band_mult;
-          st.rest_hi = st.band_hi + (st.band_hi - st.band_lo) * (float)kDeepBands;
           st.bin_inv = (float)kBins / (st.band_hi - st.band_lo);
           if (!(st.bin_inv < INFINITY)) st.bin_inv = 0.0f;
           for (int j = 0; j < kBins; ++j) {
@@ -941,10 +929,8 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
           if (st.n_buckets > kMaxBuckets) fail_query(st, VINE_ERR_TIMEOUT, kSiteRounds);
           over_time(P, st);
           st.rb_band = 0;
-          st.rb_deep = 0;
-          const float fmin =
-              __uint_as_float(min(st.far_min_bits, min(st.rest_min_bits, st.deep_min_bits)));
-          if (st.far_n == 0 && st.rest_n == 0 && st.deep_n == 0) {
+          const float fmin = __uint_as_float(min(st.far_min_bits, st.rest_min_bits));
+          if (st.far_n == 0 && st.rest_n == 0) {
             st.done = 1;
           } else if (P.mode == VINE_MODE_OPTIMAL && st.inc_key != ~0ull && fmin > key_d(st.inc_key)) {
             st.done = 1;
@@ -961,24 +947,12 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
                 st.bin_min[j] = kInfBits;
               }
               st.rb_band = 1;
-              // move the rest pile's key range on when the band has used
-              // half of it (or the rest pile ran dry)
-              const float bw = st.band_hi - st.band_lo;
-              if (st.rest_n == 0 || !(st.band_hi + bw * (float)(kDeepBands / 2) < st.rest_hi))
-                st.rb_deep = 1;
             } else if (__uint_as_float(st.rest_min_bits) < st.band_hi) {
               st.rb_band = 1;  // labels that found their bin full wait in the rest pile
             }
-            if (__uint_as_float(st.deep_min_bits) < st.band_hi) st.rb_deep = 1;  // needed now
-            if (st.deep_n == 0) st.rb_deep = 0;
             if (st.rb_band) {
               st.rest_min_bits = kInfBits;
               st.rest_wpos = 0;
-            }
-            if (st.rb_deep) {
-              st.rest_hi = st.band_hi + (st.band_hi - st.band_lo) * (float)kDeepBands;
-              st.deep_min_bits = kInfBits;
-              st.deep_wpos = 0;
             }
             float hi = fminf(st.lo + st.width, st.band_hi);
             if (!(hi > st.lo)) hi = nextafterf(st.lo, INFINITY);
@@ -1051,62 +1025,6 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(SearchParams P) {
             st.split_items += rn;
             st.rest_items += rn;
             st.rest_n = st.rest_wpos;
-          }
-          __syncthreads();
-        }
-        if (st.rb_deep) {
-          // ---- deep-pile labels: below band_hi into their bins, below the
-          // ---- rest pile's new range end onto the rest pile, the others
-          // ---- stay (compacted in place, tile by tile)
-          const uint32_t dn = st.deep_n;
-          const uint32_t dtile = (uint32_t)G * kSplitBatch;
-          for (uint32_t base = 0; base < dn; base += dtile) {
-            if (tid == 0) pool_reserve(P, st, dtile);  // for labels offered directly
-            __syncthreads();
-            if (st.abort) break;
-            Label item[kSplitBatch];
-            float f[kSplitBatch];
-#pragma unroll
-            for (int b = 0; b < kSplitBatch; ++b) {
-              const uint32_t i = base + (uint32_t)(b * G + tid);
-              if (i < dn) {
-                item[b] = c.deep[i];
-                f[b] = c.deep_key[i];
-              }
-            }
-            __syncthreads();  // the whole tile is read before it is overwritten
-#pragma unroll
-            for (int b = 0; b < kSplitBatch; ++b) {
-              if (base + (uint32_t)(b * G + tid) >= dn) break;
-              if (P.mode == VINE_MODE_OPTIMAL &&
-                  f[b] > key_d(*reinterpret_cast<volatile unsigned long long *>(&st.inc_key))) {
-                // beaten by the incumbent
-              } else if (f[b] < st.band_hi && push_bin(c, item[b], f[b])) {
-              } else if (f[b] < bucket_hi(st)) {
-                const Label &it = item[b];
-                offer(c, it.vid, it.d, it.dl, (uint32_t)it.parent, true);
-              } else if (f[b] < st.rest_hi) {
-                const uint32_t w = warp_agg_inc(&st.rest_n);
-                if (w >= (uint64_t)P.rest_cap) {
-                  fail_query(st, VINE_ERR_CAPACITY, kSiteRest);
-                } else {
-                  c.rest[w] = item[b];
-                  c.rest_key[w] = f[b];
-                  atomicMin(&st.rest_min_bits, __float_as_uint(f[b]));
-                }
-              } else {
-                const uint32_t w = warp_agg_inc(&st.deep_wpos);
-                c.deep[w] = item[b];
-                c.deep_key[w] = f[b];
-                atomicMin(&st.deep_min_bits, __float_as_uint(f[b]));
-              }
-            }
-            __syncthreads();
-          }
-          if (tid == 0) {
-            st.split_items += dn;
-            st.rest_items += dn;
-            st.deep_n = st.deep_wpos;
           }
           __syncthreads();
         }
@@ -1353,8 +1271,6 @@ void BatchWorkspace::release() {
   cudaFree(rest);
   cudaFree(far_key);
   cudaFree(rest_key);
-  cudaFree(deep);
-  cudaFree(deep_key);
   cudaFree(chunks);
   cudaFree(path_arena);
   cudaFree(path_start);
@@ -1387,8 +1303,6 @@ static int ensure_batch_workspace(vine_graph *g, const Resolved &r, int32_t nq) 
     w.rest_cap = 4 * c.far_capacity;
     VINE_CUDA_TRY(cudaMalloc(&w.rest, sizeof(Label) * (size_t)w.rest_cap * r.slots));
     VINE_CUDA_TRY(cudaMalloc(&w.rest_key, sizeof(float) * (size_t)w.rest_cap * r.slots));
-    VINE_CUDA_TRY(cudaMalloc(&w.deep, sizeof(Label) * (size_t)w.rest_cap * r.slots));
-    VINE_CUDA_TRY(cudaMalloc(&w.deep_key, sizeof(float) * (size_t)w.rest_cap * r.slots));
     w.max_chunks = 4096;
     VINE_CUDA_TRY(cudaMalloc(&w.chunks, sizeof(uint2) * (size_t)w.max_chunks * r.slots));
     VINE_CUDA_TRY(cudaMalloc(&w.sinklist, sizeof(uint32_t) * (size_t)sink_cap * r.slots));
@@ -1487,8 +1401,6 @@ int batch_enqueue(vine_graph *g, const Resolved &r, int32_t nq, const int32_t *d
   P.rest_cap = w.rest_cap;
   P.far_key = w.far_key;
   P.rest_key = w.rest_key;
-  P.deep = w.deep;
-  P.deep_key = w.deep_key;
   P.band_mult = c.band_mult;
   P.chunks = w.chunks;
   P.max_chunks = w.max_chunks;

@@ -33,8 +33,6 @@ struct BatchWorkspace {
   Label *rest = nullptr;        // per worker rest pile
   float *far_key = nullptr;     // keys beside the band bins
   float *rest_key = nullptr;    // keys beside the rest pile
-  Label *deep = nullptr;        // per worker deep pile (keys past the rest pile's range)
-  float *deep_key = nullptr;
   int64_t rest_cap = 0;
   uint2 *chunks = nullptr;      // per worker arena chunk lists
   int max_chunks = 0;

@@ -54,8 +54,6 @@ struct SearchParams {
   int64_t rest_cap;
   float *far_key;    // key f = d + h(v) of every band / rest pile entry (the
   float *rest_key;   // key is fixed for a query, so rescans need no h lookup)
-  Label *deep;       // keys >= rest_hi (beyond the rest pile's range)
-  float *deep_key;
   int band_mult;     // band width in bucket widths
   uint2 *chunks;     // per worker: arena chunks (base, size) kept across queries
   int max_chunks;
@@ -125,10 +123,7 @@ struct __align__(16) QueryState {
   uint32_t qbase, bcur;
   uint32_t far_n, far_wpos, far_min_bits;
   uint32_t rest_n, rest_wpos, rest_min_bits;
-  uint32_t deep_n, deep_wpos, deep_min_bits;
   float band_hi;
-  float rest_hi;  // the rest pile holds keys below this; the deep pile the rest
-  int rb_deep;
   uint32_t n_chunks, cur_chunk;
   int abort_site;
   int rb_band;
@@ -193,8 +188,6 @@ struct Ctx {
   Label *rest;
   float *far_key = nullptr;   // keys beside the band bins (batch engine)
   float *rest_key = nullptr;  // keys beside the rest pile (batch engine)
-  Label *deep = nullptr;      // deep pile and its keys (batch engine)
-  float *deep_key = nullptr;
   uint32_t *sinks;
   uint32_t c_dominated = 0, c_near = 0, c_far = 0, c_spills = 0, c_candidates = 0;
   unsigned long long c_idle = 0, c_publish = 0;  // warps-pull waits (lane 0 of each warp)
@@ -224,8 +217,7 @@ __device__ __forceinline__ void fail_query(QueryState &st, int status, int site)
 enum AbortSite {
   kSiteArena = 1, kSiteArenaAlloc = 2, kSiteNear = 3, kSiteBand = 4, kSiteRest = 5,
   kSiteSink = 6, kSiteLock = 7, kSiteRounds = 8, kSitePath = 9, kSiteChunks = 10,
-  kSiteInvalid = 11, kSiteAsync = 12, kSiteTime = 13, kSiteRing = 14, kSiteTile = 15,
-  kSiteDeep = 16
+  kSiteInvalid = 11, kSiteAsync = 12, kSiteTime = 13, kSiteRing = 14, kSiteTile = 15
 };  // the values of enum vine_abort_site (vine.h)
 
 // Device global timer in nanoseconds.
@@ -429,17 +421,6 @@ __device__ __forceinline__ void push_far(Ctx &c, const Label &l, float f) {
     }
     c.far[pos] = l;
     atomicMin(&st.far_min_bits, __float_as_uint(f));
-  } else if (c.deep && !(f < st.rest_hi)) {
-    // beyond the rest pile's key range: the deep pile, rescanned only when
-    // that range moves on
-    const uint32_t pos = warp_agg_inc(&st.deep_n);
-    if (pos >= (uint64_t)c.P.rest_cap) {
-      fail_query(st, VINE_ERR_CAPACITY, kSiteDeep);
-      return;
-    }
-    c.deep[pos] = l;
-    c.deep_key[pos] = f;
-    atomicMin(&st.deep_min_bits, __float_as_uint(f));
   } else {
     const uint32_t pos = warp_agg_inc(&st.rest_n);
     if (pos >= (uint64_t)c.P.rest_cap) {
