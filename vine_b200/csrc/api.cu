@@ -163,7 +163,8 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
   if (c.wait_limit == 0) c.wait_limit = 1 << 26;
   if (c.wait_limit < 1) return fail(VINE_ERR_INVALID, "wait_limit must be >= 0");
   if (c.time_limit_ms == 0) c.time_limit_ms = 600000;
-  if (c.far_capacity == 0) c.far_capacity = int64_t(1) << 20;
+  const bool far_auto = c.far_capacity == 0;
+  if (far_auto) c.far_capacity = int64_t(1) << 20;  // sized below once the worker count is known
   if (c.far_capacity < 1024 || c.far_capacity > (int64_t(1) << 30))
     return fail(VINE_ERR_INVALID, "far_capacity out of range");
   if (c.pool_labels == 0) {
@@ -189,6 +190,17 @@ int resolve_config(const vine_graph *g, const vine_config *in, Resolved *out) {
   out->round_cap = round_cap;
   out->slots = 0;
   if (c.engine == VINE_ENGINE_BATCH) VINE_TRY(batch_slots(g, c, round_cap, &out->slots));
+  if (far_auto && out->slots > 0) {
+    // every worker holds far_capacity x 160 bytes of piles (band bins and
+    // rest pile, 4 x far_capacity labels + keys each): keep them within a
+    // quarter of the device's memory, at most 2^20 per worker
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const int64_t per_worker = (int64_t)(total_b / 4 / (size_t)out->slots / 160);
+    int64_t cap = int64_t(1) << 20;
+    while (cap > 4096 && cap > per_worker) cap >>= 1;
+    c.far_capacity = cap;
+  }
   out->cfg = c;
   return VINE_OK;
 }
@@ -570,6 +582,16 @@ int vine_solve(vine_graph *g, int32_t nq, const int32_t *src, const int32_t *dst
     r.cfg.spill_log2 = std::min(r.cfg.spill_log2 + 3, 22);
     r.cfg.ctas_per_sm = 1;
     r.cfg.trace = 0;
+    {
+      // the retried workers' piles (160 bytes per far_capacity unit each)
+      // stay within a third of the device's memory
+      size_t free_b = 0, total_b = 0;
+      cudaMemGetInfo(&free_b, &total_b);
+      const int64_t workers = std::max<int64_t>(1, std::min<int64_t>(r.cfg.max_workers, (int64_t)g->sm_count));
+      while (r.cfg.far_capacity > (int64_t(1) << 20) &&
+             workers * r.cfg.far_capacity * 160 > (int64_t)(total_b / 3))
+        r.cfg.far_capacity >>= 1;
+    }
     VINE_TRY(resolve_config(g, &r.cfg, &r));
     r.chunk_log2 = 20;  // 4096 chunks of 2^20 labels per worker: room for any query the arena holds
     todo = retry;
