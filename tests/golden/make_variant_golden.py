@@ -26,12 +26,13 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[2]
 sys.path[:0] = [str(ROOT), str(ROOT / "tests")]
 
-from golden_util import load_fixture  # noqa: E402
+from golden_util import load_fixture, load_scale  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
 OUT = Path(__file__).resolve().parent / "variants.json"
 GRAPHS = ["kat3", "diamond", "line", "cycle", "road_small", "road_anticorr_small", "chunglu_small",
-          "road_batch_small"]
+          "road_batch_small", "tech_routers_rf", "tech_internet_as"]
+SCALE = {"tech_routers_rf", "tech_internet_as"}  # the reference's real graphs (full-size fixtures)
 CAP_S = 60.0
 
 
@@ -40,7 +41,7 @@ def main():
         O.build()
     out = {}
     for name in GRAPHS:
-        fx = load_fixture(name)
+        fx = load_scale(name) if name in SCALE else load_fixture(name)
         ok = (fx["src"] >= 0) & (fx["dst"] >= 0) & (fx["src"] < len(fx["row_ptr"]) - 1) & \
              (fx["dst"] < len(fx["row_ptr"]) - 1) & (fx["budget"] >= 0)
         src, dst, bud = fx["src"][ok], fx["dst"][ok], fx["budget"][ok]

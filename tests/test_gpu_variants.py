@@ -13,7 +13,7 @@ import json
 import numpy as np
 import pytest
 
-from golden_util import GOLDEN, check_result, load_fixture
+from golden_util import GOLDEN, check_result, load_fixture, load_scale
 
 pytestmark = pytest.mark.gpu
 
@@ -48,7 +48,7 @@ def graphs():
         if name not in cache:
             for old in list(cache):
                 cache.pop(old)[1].close()
-            fx = load_fixture(name)
+            fx = load_scale(name) if name.startswith("tech_") else load_fixture(name)
             cache[name] = (fx, v.Graph(fx["row_ptr"], fx["col"], fx["len"], fx["delay"]))
         return cache[name]
     yield get
