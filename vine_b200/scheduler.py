@@ -123,32 +123,40 @@ def train(x, y, device: int = 0, epochs: int = 30, batch: int = 512, lr: float =
     return mlp, float(loss0), float(loss)
 
 
-def evaluate(graph: v.Graph, src, dst, budget, mean_len: float, mlp, repeats: int = 3,
+def evaluate(graph: v.Graph, src, dst, budget, mean_len: float, mlp, repeats: int = 5,
              answers=None, warm_up: bool = True):
     """Times the batch engine under the fixed, AR and MLP policies (same base
     width); returns {policy: {ms, cycles, expanded}} and checks every arm
-    returns identical costs."""
+    returns identical costs.  The arms are interleaved (fixed, AR, MLP,
+    fixed, AR, ...) and each arm's time is the median of its runs, so a
+    drift of the machine's speed during the evaluation does not favour one
+    arm."""
     import torch
     out = {}
-    ref = answers
     arms = {"fixed": base_config(mean_len, policy="fixed"),
             "ar": base_config(mean_len, policy="ar")}
     if mlp is not None:
         arms["mlp"] = base_config(mean_len, policy="mlp", mlp=mlp)
-    for name, cfg in arms.items():
-        if warm_up:
+    if warm_up:
+        for cfg in arms.values():
             v.solve(graph, src, dst, budget, cfg, paths=False)
-        times = []
-        for _ in range(repeats):
+    times = {name: [] for name in arms}
+    last = {}
+    for _ in range(repeats):
+        for name, cfg in arms.items():
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             r = v.solve(graph, src, dst, budget, cfg, paths=False, stats=True)
-            times.append((time.perf_counter() - t0) * 1e3)
+            times[name].append((time.perf_counter() - t0) * 1e3)
+            last[name] = r
+    ref = answers
+    for name, r in last.items():
         if ref is None:
             ref = (r.cost.copy(), r.found.copy())
         same = bool(np.array_equal(r.found, ref[1]) and
                     np.array_equal(np.where(r.found == 1, r.cost, 0), np.where(ref[1] == 1, ref[0], 0)))
-        out[name] = {"ms": float(np.median(times)), "ms_all": [round(t, 1) for t in times],
+        out[name] = {"ms": float(np.median(times[name])),
+                     "ms_all": [round(t, 1) for t in times[name]],
                      "retried": int(r.retried),
                      "cycles": float(r.stats[:, STAT_CYCLES].sum()),
                      "cycles_max": float(r.stats[:, STAT_CYCLES].max()),
@@ -181,7 +189,7 @@ def _evaluate_batch(a, mlp, config: int):
     # the 1.5M-vertex batch takes minutes per arm: one timed run each
     heavy = config == 3
     res = evaluate(ge, ev.src, ev.dst, ev.budget, float(ev.len.mean()), mlp,
-                   repeats=1 if heavy else 3, warm_up=not heavy)
+                   repeats=1 if heavy else 5, warm_up=not heavy)
     ge.close()
     return res, n
 
@@ -225,10 +233,12 @@ def main(argv=None):
             raise SystemExit("no trained scheduler to evaluate")
         ev = _evaluate_all(a, mlp)
         first = ev[str(a.eval_configs[0])]
+        by_config = dict(meta.get("eval_by_config", {}))
+        by_config.update(ev)  # configs not re-evaluated keep their record
         meta.update({"eval_config": a.eval_configs[0], "eval_queries": first["queries"],
                      "eval_seed": a.eval_seed,
                      "eval": {k: v_ for k, v_ in first.items() if k != "queries"},
-                     "eval_by_config": ev})
+                     "eval_by_config": by_config})
         MODEL_JSON.write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
         text = json.dumps(meta, indent=1, sort_keys=True)
         if a.out:
