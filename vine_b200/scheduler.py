@@ -221,6 +221,10 @@ def main(argv=None):
     ap.add_argument("--eval-only", action="store_true",
                     help="re-evaluate the committed network without training")
     ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--margin", type=float, default=MARGIN,
+                    help="share of a query's cycles another multiplier must save to be its label")
+    ap.add_argument("--model-dir", default=None,
+                    help="write the network and its record here instead of vine_b200/models")
     ap.add_argument("--out", default=None, help="write the evaluation JSON here")
     a = ap.parse_args(argv)
     a.eval_configs = [int(x) for x in a.eval_configs.split(",") if x]
@@ -256,7 +260,7 @@ def main(argv=None):
         g = wl.graph()
         cycles, traces, settings = collect(g, wl.src, wl.dst, wl.budget, float(wl.len.mean()))
         g.close()
-        x, y = make_dataset(cycles, traces, settings)
+        x, y = make_dataset(cycles, traces, settings, margin=a.margin)
         xs.append(x)
         ys.append(y)
         best = np.argmin(cycles, axis=0)
@@ -279,7 +283,8 @@ def main(argv=None):
     ev = _evaluate_all(a, mlp)
     first = ev[str(a.eval_configs[0])]
     meta = {"base_mult": BASE_MULT, "table_log2": TABLE_LOG2, "block_threads": 512,
-            "margin": MARGIN, "train_configs": a.train_configs, "rows": int(x.shape[0]),
+            "margin": a.margin, "train_configs": a.train_configs, "rows": int(x.shape[0]),
+            "train_queries_c5": a.train_queries,
             "loss_initial": loss0, "loss_final": loss, "epochs": a.epochs,
             "training": per_config,
             "eval_config": a.eval_configs[0], "eval_queries": first["queries"],
@@ -287,7 +292,13 @@ def main(argv=None):
             "eval": {k: v_ for k, v_ in first.items() if k != "queries"},
             "eval_by_config": ev,
             "seconds": time.time() - t0}
-    save(mlp, meta)
+    if a.model_dir:
+        d = Path(a.model_dir)
+        d.mkdir(parents=True, exist_ok=True)
+        np.save(d / MODEL_NPY.name, mlp.params)
+        (d / MODEL_JSON.name).write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
+    else:
+        save(mlp, meta)
     text = json.dumps(meta, indent=1, sort_keys=True)
     if a.out:
         Path(a.out).write_text(text + "\n")
