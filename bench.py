@@ -165,7 +165,13 @@ def scheduler_record() -> dict:
     ev = meta.get("eval", {})
     if not all(k in ev for k in ("ar", "mlp", "fixed")):
         return {}
-    return {"mlp_faster": ev["mlp"]["ms"] < ev["ar"]["ms"],
+    # the network drives the headline only when its median batch time beats
+    # the AR rule's and none of its runs was more than 2 % slower than the
+    # AR rule's slowest (a learned policy must not bring a worse tail)
+    tail_ok = max(ev["mlp"].get("ms_all", [ev["mlp"]["ms"]])) <= \
+        1.02 * max(ev["ar"].get("ms_all", [ev["ar"]["ms"]]))
+    return {"mlp_faster": ev["mlp"]["ms"] < ev["ar"]["ms"] and tail_ok,
+            "mlp_median_faster": ev["mlp"]["ms"] < ev["ar"]["ms"], "mlp_tail_ok": tail_ok,
             "heldout_queries": meta.get("eval_queries"),
             "mlp_vs_ar_sm_cycles": ev["mlp"]["cycles"] / ev["ar"]["cycles"],
             "mlp_vs_ar_batch_ms": ev["mlp"]["ms"] / ev["ar"]["ms"],

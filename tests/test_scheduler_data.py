@@ -39,3 +39,26 @@ def test_rows_with_non_finite_features_are_dropped():
     x, y = S.make_dataset(np.array([[1.0], [1.0], [1.0]]), tr, [0.5, 1.0, 2.0],
                           rows_per_setting=500, seed=2)
     assert np.isfinite(x).all() and np.isfinite(y).all() and x.shape[0] > 0
+
+
+def test_auto_policy_needs_a_faster_median_and_no_worse_tail(tmp_path, monkeypatch):
+    import json
+    import bench
+    from vine_b200 import scheduler as S
+
+    def record(mlp_runs, ar_runs):
+        def arm(runs):
+            return {"ms": float(np.median(runs)), "ms_all": runs, "cycles": 1.0}
+        meta = {"eval": {"fixed": arm([3000.0]), "ar": arm(ar_runs), "mlp": arm(mlp_runs)}}
+        path = tmp_path / "m.json"
+        path.write_text(json.dumps(meta))
+        monkeypatch.setattr(S, "MODEL_JSON", path)
+        monkeypatch.setattr(bench, "MODEL_PATH", path)
+        return bench.scheduler_record()
+
+    r = record([1600.0, 1610.0, 1620.0], [1670.0, 1671.0, 1672.0])
+    assert r["mlp_faster"] and r["mlp_tail_ok"]
+    r = record([1600.0, 1610.0, 5774.0], [1670.0, 1671.0, 1672.0])   # one blown-up run
+    assert r["mlp_median_faster"] and not r["mlp_tail_ok"] and not r["mlp_faster"]
+    r = record([1690.0, 1690.0, 1690.0], [1670.0, 1671.0, 1672.0])   # slower median
+    assert r["mlp_tail_ok"] and not r["mlp_faster"]
