@@ -348,17 +348,36 @@ __device__ __forceinline__ InsertResult table_insert_locked(const BucketTable &b
   if (!had_free) {
     bep = vs->bep;
     if (bep == bt.bcur) {
-      uint32_t steps = 0;
-      for (uint32_t k = vs->bhead; k != kNone; k = __ldcg(&bt.next[k])) {
+      // Dead labels are unlinked as the walk meets them (only the holder of
+      // v's stripe lock walks or changes v's chain), so a vertex that takes
+      // many labels in one wide bucket keeps a chain of its live labels, not
+      // of every label it ever held.  bmin keeps the dead labels' delays:
+      // each was dominated by a label of the same bucket with a delay no
+      // larger, so the settled delay of v is unchanged.
+      uint32_t steps = 0, prev = kNone;
+      for (uint32_t k = vs->bhead; k != kNone;) {
         ++steps;
+        const uint32_t nk = __ldcg(&bt.next[k]);
         const int4 raw = __ldcg(reinterpret_cast<const int4 *>(&pool[k]));
-        if (raw.x & (int)kDeadBit) continue;
-        bool kill;
-        if (check_one(__int_as_float(raw.y), __int_as_float(raw.z), d, dl, &kill)) {
-          if (bt.chain_steps) atomicAdd(bt.chain_steps, (unsigned long long)steps);
-          return kDominated;
+        bool dead = (raw.x & (int)kDeadBit) != 0;
+        if (!dead) {
+          bool kill;
+          if (check_one(__int_as_float(raw.y), __int_as_float(raw.z), d, dl, &kill)) {
+            if (bt.chain_steps) atomicAdd(bt.chain_steps, (unsigned long long)steps);
+            return kDominated;
+          }
+          if (kill) {
+            atomicOr(reinterpret_cast<unsigned int *>(&pool[k].vid), kDeadBit);
+            dead = true;
+          }
         }
-        if (kill) atomicOr(reinterpret_cast<unsigned int *>(&pool[k].vid), kDeadBit);
+        if (dead) {
+          if (prev == kNone) vs->bhead = nk;
+          else __stcg(&bt.next[prev], nk);
+        } else {
+          prev = k;
+        }
+        k = nk;
       }
       if (bt.chain_steps) atomicAdd(bt.chain_steps, (unsigned long long)steps);
     }

@@ -705,6 +705,7 @@ __device__ __forceinline__ float reverse_dist(const Ctx &c, int which, int v) {
 // keeps the search exact), with the AR rule as fallback.
 __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
   const int lane = threadIdx.x & 31;
+  const float prev_width = st.width;  // the width the finished bucket was opened with
   if (lane == 0) {
     const double xs = log2(1.0 + (double)st.b_labels);
     if (st.hist_n < kHist) {
@@ -784,6 +785,12 @@ __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
       // rule's width stands.
       if (isfinite(y0) && isfinite(y1) && y1 > 0.5f)
         st.width = st.ar_width * exp2f(fminf(fmaxf(y0, -1.5f), 1.5f));
+      // While the network narrows the buckets, their sizes fall and the AR
+      // rule's own width widens (its "ending" step); when the gate then
+      // closes, that width would open one bucket many times the table's
+      // size, whose spills cost more than the network ever saves.  So the
+      // width grows by at most 2x a bucket, the AR rule's own largest step.
+      st.width = fminf(st.width, 2.0f * prev_width);
     }
     __syncwarp();
   }
