@@ -47,7 +47,7 @@ from . import api as v
 
 SCALES = (0.35, 0.5, 0.7, 1.0, 1.4, 2.0, 2.8)  # multipliers on the AR width
 BASE_MULT = 0.3          # initial bucket width / mean arc length
-MARGIN = 0.05            # a multiplier other than 1 must save this share of a query's cycles
+MARGIN = 0.03            # a multiplier other than 1 must save this share of a query's cycles
 TABLE_LOG2 = 13
 MODEL_DIR = Path(__file__).resolve().parent / "models"
 MODEL_NPY = MODEL_DIR / "scheduler_mlp.npy"
@@ -206,7 +206,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--train-configs", default="1,2,5",
                     help="workloads whose traces train the network")
-    ap.add_argument("--train-queries", type=int, default=1024,
+    ap.add_argument("--train-queries", type=int, default=4096,
                     help="queries of the config-5 training batch")
     ap.add_argument("--train-queries-c3", type=int, default=48,
                     help="queries of a config-3 training batch (own query seed), when 3 is "
