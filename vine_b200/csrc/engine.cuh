@@ -68,8 +68,14 @@ struct VView {
 // qbase / bcur: first bucket id of the query and id of the open bucket.
 __device__ __forceinline__ VView view_vs(const VState *p, uint32_t epoch, uint32_t qbase,
                                          uint32_t bcur, bool bounds) {
-  const uint4 a = __ldcg(reinterpret_cast<const uint4 *>(p));
-  const uint4 b = __ldcg(reinterpret_cast<const uint4 *>(p) + 1);
+  // the whole 32-byte state in one 256-bit load (L2, like __ldcg); VState
+  // is 32-byte aligned
+  uint4 a, b;
+  asm volatile("ld.global.cg.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z),
+                 "=r"(b.w)
+               : "l"(p)
+               : "memory");
   VView v;
   float sd = a.x == epoch ? __uint_as_float(a.y) : INFINITY;
   if (b.x >= qbase && b.x < bcur) sd = fminf(sd, __uint_as_float(b.y));
