@@ -62,3 +62,33 @@ def test_auto_policy_needs_a_faster_median_and_no_worse_tail(tmp_path, monkeypat
     assert r["mlp_median_faster"] and not r["mlp_tail_ok"] and not r["mlp_faster"]
     r = record([1690.0, 1690.0, 1690.0], [1670.0, 1671.0, 1672.0])   # slower median
     assert r["mlp_tail_ok"] and not r["mlp_faster"]
+
+
+def test_trainer_defaults_reproduce_the_shipped_network_recipe():
+    """`python -m vine_b200.scheduler` with no options trains the network the
+    way the committed one was trained (its record holds the recipe)."""
+    import json
+    from vine_b200 import scheduler as S
+    meta = json.loads(S.MODEL_JSON.read_text())
+    assert S.MARGIN == meta["margin"]
+    parser_defaults = {}
+    import argparse
+    orig = argparse.ArgumentParser.parse_args
+
+    def capture(self, argv=None, namespace=None):
+        ns = orig(self, [], namespace)
+        parser_defaults.update(vars(ns))
+        raise SystemExit(0)
+    try:
+        argparse.ArgumentParser.parse_args = capture
+        try:
+            S.main([])
+        except SystemExit:
+            pass
+    finally:
+        argparse.ArgumentParser.parse_args = orig
+    assert parser_defaults["margin"] == meta["margin"]
+    assert parser_defaults["train_queries"] == meta["train_queries_c5"]
+    assert [int(x) for x in parser_defaults["train_configs"].split(",")] == meta["train_configs"]
+    assert parser_defaults["epochs"] == meta["epochs"]
+    assert parser_defaults["eval_seed"] == meta["eval_seed"]
