@@ -10,6 +10,8 @@
 // far, so every device gets a similar mix of heavy and light queries.
 
 #include <algorithm>
+#include <climits>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <numeric>
@@ -21,6 +23,10 @@
 #include "common.h"
 
 using namespace vine;
+
+namespace {
+constexpr int32_t kUnset = INT32_MIN;  // per-query status not written by the call
+}
 
 extern "C" {
 
@@ -80,10 +86,12 @@ int vine_solve_multi(vine_graph **graphs, int32_t ngraphs, int32_t nq, const int
         x.t[i] = dst[idx[i]];
         x.b[i] = budget[idx[i]];
       }
-      x.cost.resize(n);
-      x.delay.resize(n);
-      x.found.resize(n);
-      x.status.resize(n);
+      // a call that fails before it writes the per-query outputs leaves
+      // these: not found, and (below) the call's own status
+      x.cost.assign(n, INFINITY);
+      x.delay.assign(n, INFINITY);
+      x.found.assign(n, 0);
+      x.status.assign(n, kUnset);
       vine_results r = {};
       r.cost = x.cost.data();
       r.delay = x.delay.data();
@@ -117,6 +125,8 @@ int vine_solve_multi(vine_graph **graphs, int32_t ngraphs, int32_t nq, const int
       }
       x.retried = r.retried;
       if (x.rc != VINE_OK) x.err = vine_last_error();
+      for (int32_t &st : x.status)
+        if (st == kUnset) st = x.rc;
     });
   }
   for (auto &t : th) t.join();
