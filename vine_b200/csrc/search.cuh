@@ -705,8 +705,9 @@ __device__ __forceinline__ float reverse_dist(const Ctx &c, int which, int v) {
 // keeps the search exact), with the AR rule as fallback.
 __device__ inline void policy_step(const SearchParams &P, QueryState &st) {
   const int lane = threadIdx.x & 31;
-  const float prev_width = st.width;  // the width the finished bucket was opened with
+  float prev_width = 0.0f;  // the width the finished bucket was opened with (lane 0)
   if (lane == 0) {
+    prev_width = st.width;
     const double xs = log2(1.0 + (double)st.b_labels);
     if (st.hist_n < kHist) {
       st.hist[st.hist_n++] = xs;
