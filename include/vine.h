@@ -279,7 +279,11 @@ int vine_solve_labels(vine_graph *g, int32_t kind, int32_t nq, const int32_t *sr
  * sets (pareto_d / pareto_delay / pareto_n / pareto_stride) of out.
  * nthreads 0 = all cores; across_queries = 0 runs the queries one after the
  * other, each expanded by all threads (as the reference does); 1 gives each
- * thread its own queries.  Same answers either way and for every nthreads. */
+ * thread its own queries.  Same answers either way and for every nthreads.
+ * A query that would hold more labels than a cap (a quarter of physical
+ * memory shared by the queries in flight, about 96 bytes a label; the
+ * environment variable VINE_HOST_MAX_LABELS, read per call, overrides it)
+ * stops with status VINE_ERR_CAPACITY and no answer; the others finish. */
 int vine_solve_host(int32_t n, int64_t m, const int64_t *row_ptr, const int32_t *col,
                     const float *len, const float *delay, int32_t nq, const int32_t *src,
                     const int32_t *dst, const float *budget, int32_t nthreads,

@@ -62,3 +62,27 @@ def test_cspp_solve_omp_and_cpu():
             assert bool(s.found_l[q]) == e["found"]
             if e["found"]:
                 assert float(s.cost_l[q]) == e["cost"] and s.size_of_result_l[q] >= 1
+
+
+def test_host_engine_label_cap_fails_the_query_not_the_host(monkeypatch):
+    """A query that would hold more labels than the cap stops with
+    VINE_ERR_CAPACITY and no answer; small queries of the same call finish
+    exactly (the cap is forced low through VINE_HOST_MAX_LABELS)."""
+    import vine_b200 as v
+    fx = load_fixture("road_small")
+    g = v.Graph(fx["row_ptr"], fx["col"], fx["len"], fx["delay"])
+    full = v.solve_host(g, fx["src"], fx["dst"], fx["budget"], nthreads=2, raise_on_error=False)
+    monkeypatch.setenv("VINE_HOST_MAX_LABELS", "200")
+    for across in (False, True):
+        res = v.solve_host(g, fx["src"], fx["dst"], fx["budget"], nthreads=2, across_queries=across,
+                           raise_on_error=False)
+        capped = res.status == v._lib.VINE_ERR_CAPACITY
+        assert capped.any() and not capped.all()
+        assert (res.found[capped] == 0).all()
+        ok = res.status == 0
+        assert np.array_equal(res.found[ok], full.found[ok])
+        assert np.array_equal(np.where(res.found[ok] == 1, res.cost[ok], 0),
+                              np.where(full.found[ok] == 1, full.cost[ok], 0))
+    monkeypatch.delenv("VINE_HOST_MAX_LABELS")
+    again = v.solve_host(g, fx["src"], fx["dst"], fx["budget"], nthreads=2, raise_on_error=False)
+    assert np.array_equal(again.status, full.status)

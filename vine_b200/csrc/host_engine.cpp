@@ -19,7 +19,15 @@
 //
 // Every list is touched by its owner only, so the run is race-free and the
 // result does not depend on the thread count: the sink list ends as the set
-// of non-dominated feasible sink labels.  Labels carry their parent (a
+// of non-dominated feasible sink labels.
+//
+// One change of the reference's rule: a label erased from its vertex's list
+// (dominated by a later arrival) is marked dead and not expanded when its
+// round comes.  The reference expands it all the same, and how many such
+// labels a round holds depends on the order children arrive in; on a 100x100
+// grid one thread (breadth-first order) expanded some 20x more labels than
+// two.  Skipping them is exact: the dominating label is in the frontier too,
+// and its child over each arc dominates the dead label's child over it.  Labels carry their parent (a
 // (thread, index) arena reference), so the answer's path is returned too.
 // The answer is the lexicographically smallest (cost, delay) label of the
 // sink's list, as for the GPU engines.
@@ -29,6 +37,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <limits>
@@ -36,6 +45,8 @@
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <unistd.h>
 
 #include "../../include/vine.h"
 #include "common.h"
@@ -58,6 +69,7 @@ inline bool hdom(const HLabel &a, const HLabel &b) {  // include/label.hpp:244-2
 struct Node {
   int32_t vid;
   int64_t parent;
+  bool dead;  // erased from its vertex's list: dominated, not expanded
 };
 
 // Runs fn(t) on T threads and waits for all of them (threads kept between rounds).
@@ -130,20 +142,27 @@ struct QueryOut {
   std::vector<std::pair<float, float>> pareto;
 };
 
-// One query with T threads (pool may be null when T == 1).
-void solve_one(const HostGraph &g, int32_t s, int32_t t, float L, int T, RoundPool *pool,
-               QueryOut *out) {
+// One query with T threads (pool may be null when T == 1).  Returns
+// VINE_ERR_CAPACITY, with no answer, once the query holds more than
+// max_labels labels (checked after every round), else VINE_OK.
+int solve_one(const HostGraph &g, int32_t s, int32_t t, float L, int T, RoundPool *pool,
+              int64_t max_labels, QueryOut *out) {
   const int32_t n = g.n;
   std::vector<std::vector<HLabel>> lists((size_t)n);
   std::vector<std::vector<Node>> arena((size_t)T);
   std::vector<HLabel> frontier, next;
+  auto node = [&arena](int64_t r) -> Node & {
+    return arena[(size_t)(r >> 40)][(size_t)(r & ((int64_t(1) << 40) - 1))];
+  };
   // outbox[producer][owner]: children with their parent references
   std::vector<std::vector<std::vector<std::pair<HLabel, int64_t>>>> outbox(
       (size_t)T, std::vector<std::vector<std::pair<HLabel, int64_t>>>((size_t)T));
   std::vector<std::vector<HLabel>> next_part((size_t)T);
 
-  arena[0].push_back({s, -1});
-  HLabel src{s, 0.0f, 0.0f, 0};
+  // every label at v lives in the arena of v's owner, which alone writes it
+  const int so = (int)(s % T);
+  arena[(size_t)so].push_back({s, -1, false});
+  HLabel src{s, 0.0f, 0.0f, (int64_t)so << 40};
   frontier.push_back(src);
   // the source label is stored at s, as a label of the search (a later
   // label at s with cost and delay >= 0 is dominated by it)
@@ -152,6 +171,7 @@ void solve_one(const HostGraph &g, int32_t s, int32_t t, float L, int T, RoundPo
     for (auto &box : outbox[(size_t)th]) box.clear();
     for (size_t i = (size_t)th; i < frontier.size(); i += (size_t)T) {
       const HLabel &f = frontier[i];
+      if (node(f.ref).dead) continue;  // dominated since it joined the frontier
       for (int64_t j = g.row[f.vid]; j < g.row[f.vid + 1]; ++j) {
         const int32_t v = g.col[j];
         HLabel c{v, f.d + g.len[j], f.dl + g.dly[j], -1};  // include/label.hpp:214-222
@@ -172,12 +192,16 @@ void solve_one(const HostGraph &g, int32_t s, int32_t t, float L, int T, RoundPo
             dominated = true;
             break;
           }
-          if (hdom(c, *it)) it = lst.erase(it);
-          else ++it;
+          if (hdom(c, *it)) {
+            node(it->ref).dead = true;  // v's owner is this thread: its own arena
+            it = lst.erase(it);
+          } else {
+            ++it;
+          }
         }
         if (dominated) continue;
         c.ref = ((int64_t)o << 40) | (int64_t)arena[(size_t)o].size();
-        arena[(size_t)o].push_back({c.vid, item.second});
+        arena[(size_t)o].push_back({c.vid, item.second, false});
         lst.push_back(c);
         next_part[(size_t)o].push_back(c);
       }
@@ -194,6 +218,9 @@ void solve_one(const HostGraph &g, int32_t s, int32_t t, float L, int T, RoundPo
     next.clear();
     for (int o = 0; o < T; ++o) next.insert(next.end(), next_part[(size_t)o].begin(), next_part[(size_t)o].end());
     frontier.swap(next);
+    int64_t held = 0;
+    for (const auto &a : arena) held += (int64_t)a.size();
+    if (held > max_labels) return VINE_ERR_CAPACITY;
   }
   // answer: lexicographically smallest (cost, delay) of the sink's list
   const auto &sl = lists[(size_t)t];
@@ -204,7 +231,7 @@ void solve_one(const HostGraph &g, int32_t s, int32_t t, float L, int T, RoundPo
     if (!best || l.d < best->d || (l.d == best->d && l.dl < best->dl)) best = &l;
   }
   std::sort(out->pareto.begin(), out->pareto.end());
-  if (!best) return;
+  if (!best) return VINE_OK;
   out->found = true;
   out->cost = best->d;
   out->delay = best->dl;
@@ -214,6 +241,20 @@ void solve_one(const HostGraph &g, int32_t s, int32_t t, float L, int T, RoundPo
     r = nd.parent;
   }
   std::reverse(out->path.begin(), out->path.end());
+  return VINE_OK;
+}
+
+// Labels one query may hold: a quarter of physical memory shared by the
+// queries in flight, at about 96 bytes a label (arena node, list entry,
+// frontier and outbox copies).  VINE_HOST_MAX_LABELS overrides it.
+int64_t label_cap(int in_flight) {
+  if (const char *e = std::getenv("VINE_HOST_MAX_LABELS")) {
+    const long long v = std::atoll(e);
+    if (v > 0) return (int64_t)v;
+  }
+  const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGE_SIZE);
+  const double bytes = pages > 0 && page > 0 ? (double)pages * (double)page : 16e9;
+  return std::max<int64_t>(int64_t(1) << 20, (int64_t)(bytes / 4.0 / std::max(1, in_flight) / 96.0));
 }
 
 }  // namespace
@@ -239,6 +280,7 @@ int vine_solve_host(int32_t n, int64_t m, const int64_t *row_ptr, const int32_t 
   const HostGraph g{n, row_ptr, col, len, delay};
   std::vector<QueryOut> res((size_t)nq);
   std::vector<int32_t> status((size_t)nq, VINE_OK);
+  const int64_t cap = label_cap(across_queries ? std::min<int>(T, std::max(nq, 1)) : 1);
   auto one = [&](int32_t q, int threads, RoundPool *pool) {
     const int32_t s = src[q], t = dst[q];
     const float L = budget[q];
@@ -247,7 +289,11 @@ int vine_solve_host(int32_t n, int64_t m, const int64_t *row_ptr, const int32_t 
       return;
     }
     if (0.0f > L) return;  // even the source label violates the budget
-    solve_one(g, s, t, L, threads, pool, &res[(size_t)q]);
+    const int rc = solve_one(g, s, t, L, threads, pool, cap, &res[(size_t)q]);
+    if (rc != VINE_OK) {
+      res[(size_t)q] = QueryOut();  // no partial answer
+      status[(size_t)q] = rc;
+    }
   };
   if (across_queries) {
     // one query per thread at a time, each expanded by that thread alone
@@ -264,10 +310,14 @@ int vine_solve_host(int32_t n, int64_t m, const int64_t *row_ptr, const int32_t 
   }
   int rc = VINE_OK;
   int64_t run = 0;
-  int32_t n_failed = 0;
-  for (int32_t q = 0; q < nq; ++q) n_failed += status[(size_t)q] != VINE_OK;
-  if (n_failed)
-    set_error(std::to_string(n_failed) + " of " + std::to_string(nq) + " queries are invalid");
+  int32_t n_invalid = 0, n_capacity = 0;
+  for (int32_t q = 0; q < nq; ++q) {
+    n_invalid += status[(size_t)q] == VINE_ERR_INVALID;
+    n_capacity += status[(size_t)q] == VINE_ERR_CAPACITY;
+  }
+  if (n_invalid || n_capacity)
+    set_error(std::to_string(n_invalid) + " of " + std::to_string(nq) + " queries are invalid, " +
+              std::to_string(n_capacity) + " exceeded the label cap of " + std::to_string(cap));
   for (int32_t q = 0; q < nq; ++q) {
     const QueryOut &r = res[(size_t)q];
     out->cost[q] = r.found ? r.cost : INFINITY;
