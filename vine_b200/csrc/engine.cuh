@@ -56,6 +56,9 @@ struct __align__(32) VState {
   float hlen;
   uint32_t bhead;
 };
+// view_vs reads a state with one 256-bit load, which needs exactly this
+// size and alignment (arrays of VState then keep every element aligned).
+static_assert(sizeof(VState) == 32 && alignof(VState) == 32, "VState must be one aligned 32-byte sector");
 
 // What one query sees of a vertex.
 struct VView {
